@@ -1,0 +1,99 @@
+"""The compiler restatement emits the same QSV2 programs as the reference compiler.
+
+Fixtures (tests/golden/streams.json) were produced by running the reference's host/sv/compiler.py on the
+grid of tests/test_compiler_model.py:17-27 (n in {5,7,9}; P in {1,2,4}; k in {3,4,5}; fuse; tiling; initial
+map) -- see tests/golden/make_golden.py. Comparison is exact: sha256 over every segment's int32 words
+and every remap permutation, plus the final qubit map and the pass/remap/op counts.
+"""
+import hashlib
+import itertools
+import json
+import os
+
+import numpy as np
+import pytest
+
+import qsv_b200 as q
+from qsv_b200 import generators as gen
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def prog_sha(prog):
+    h = hashlib.sha256()
+    for kind, payload in prog:
+        h.update(b"S" if kind == "segment" else b"R")
+        h.update(np.ascontiguousarray(payload, dtype=np.int32).tobytes())
+    return h.hexdigest()
+
+
+def _circuits(n):
+    out = [gen.zoo(n, s) for s in range(4)]
+    out += [gen.make(f, n) for f in ("ghz", "qft", "rqc", "vqe")]
+    out += [gen.random_layer(n, 6, 100 + n), gen.random_layer_ccx(n, 4, 200 + n)]
+    if n <= 9:
+        out.append(gen.grover(n))
+    return out
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return json.load(open(os.path.join(GOLD, "streams.json")))
+
+
+def test_streams_match_reference(golden):
+    recs = {(r["circuit"], r["P"], r["k"], r["fuse"], r["tiling"], r["init"]): r for r in golden["records"]}
+    checked = 0
+    for n in (5, 7, 9):
+        for qc in _circuits(n):
+            for P, k, fuse, tiling in itertools.product((1, 2, 4), (3, 4, 5), (True, False), (True, False)):
+                L = n - int(np.log2(P))
+                if k > L:
+                    continue
+                for init in (None, list(range(n))[::-1]):
+                    rec = recs[(qc.name, P, k, fuse, tiling, init is not None)]
+                    if "error" in rec:
+                        with pytest.raises(Exception) as ei:
+                            q.compile_circuit(qc, L, k, fuse_1q=fuse, tiling=tiling, initial_map=init)
+                        assert type(ei.value).__name__ == rec["error"]
+                        continue
+                    prog, fmap, st = q.compile_circuit(qc, L, k, fuse_1q=fuse, tiling=tiling, initial_map=init)
+                    assert prog_sha(prog) == rec["sha"], (qc.name, P, k, fuse, tiling, init)
+                    assert list(fmap) == rec["final_map"]
+                    for key, val in rec["stats"].items():
+                        assert getattr(st, key) == val, (key, qc.name)
+                    if "words" in rec:
+                        for (kind, payload), (gk, gw) in zip(prog, rec["words"]):
+                            assert kind == gk
+                            assert [int(x) for x in payload] == gw
+                    checked += 1
+    assert checked == sum(1 for r in golden["records"] if "error" not in r)
+
+
+def test_stream_header_and_records():
+    qc = gen.random_layer(10, 3, 5)
+    prog, fmap, st = q.compile_circuit(qc, 10, 8)
+    seg = prog[0][1]
+    assert seg.dtype == np.int32
+    assert seg[0] == q.isa.MAGIC and seg[1] == 10 and seg[3] == 8
+    assert seg[2] == st.n_passes
+    pos = q.isa.HDR_WORDS
+    nops = 0
+    for _ in range(int(seg[2])):
+        m, nop = int(seg[pos]), int(seg[pos + 3])
+        assert 0 <= m <= 4 and 1 <= nop <= q.isa.MAX_OPS_PER_PASS
+        pos += q.isa.PASS_WORDS
+        for _ in range(nop):
+            assert seg[pos] == q.isa.OP_MUX2
+            assert 0 <= seg[pos + 1] < 8
+            assert not (int(seg[pos + 2]) >> int(seg[pos + 1])) & 1
+            pos += q.isa.OP_WORDS
+        nops += nop
+    assert pos == len(seg) and nops == st.n_ops
+
+
+def test_unsupported_wide_gate_raises():
+    qc = q.Circuit(4)
+    qc.append("rccx_dense_unknown", (0, 1, 2))
+    with pytest.raises(KeyError):
+        q.compile_circuit(qc, 4, 4)

@@ -1,0 +1,332 @@
+"""Host compiler: circuit -> MUX2 ops -> passes -> QSV2 segments.
+
+This is the front end of the hot path. It follows the reference compiler (host/sv/compiler.py) step for
+step, because the program it emits (which ops, in which order, grouped into which passes, encoded into
+which words) defines the arithmetic the engine performs; the same circuit compiled here and by the
+reference yields the same QSV2 words (the golden-stream tests check this word for word). It does not use
+Qiskit: gate matrices come from ``gates.py`` and wide gates are lowered by ``_lower`` below instead of
+``qiskit.transpile``.
+
+Program = list of steps, executed in order by the runtime:
+  ("segment", int32 words)  one engine launch (every pass of the segment over the whole state)
+  ("remap", perm)           qubit permutation, perm[new_phys] = old_phys
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.linalg import cossin
+
+from .isa import MAGIC, OP_MUX2, MAX_OPS_PER_PASS, MAX_HIGH
+from .gates import I2, X, Z, gate_matrix, mc_matrix, phase
+from .circuit import normalize
+
+SKIP = {"measure", "barrier", "delay", "save_statevector", "id"}   # compiler.py:20
+# multi-controlled gates built directly as one MUX2 (controls all-ones select U), compiler.py:25-29
+MC_NAMES = {"ccx", "c3x", "c4x", "mcx", "mcx_gray", "mcx_recursive", "ccz", "mcphase", "mcp"}
+MAX_DENSE_QUBITS = 10     # wider gates are never expanded to a dense matrix (compiler.py:132)
+
+
+@dataclass
+class Op:
+    """One MUX2 record before encoding: target storage qubit ``t``, control storage qubits ``ctrls``
+    (all set -> M1), 2x2 matrices M0 / M1 in complex128 (compiler.py:33-42)."""
+    t: int
+    ctrls: tuple
+    M0: np.ndarray
+    M1: np.ndarray
+    src: object = None
+
+    @property
+    def q(self):
+        return (self.t,) + tuple(self.ctrls)
+
+
+@dataclass
+class Stats:
+    """Per-circuit compile statistics; the field names are the reference's (compiler.py:45-56) so the
+    runtime's ``stats`` dictionary reads the same."""
+    n_input_gates: int = 0
+    native: dict = field(default_factory=dict)
+    relabel: int = 0
+    lowered: dict = field(default_factory=dict)
+    csd_2q: int = 0
+    fused_1q: int = 0
+    n_ops: int = 0
+    n_passes: int = 0
+    n_remaps: int = 0
+    n_segments: int = 0
+
+
+def _count(d, key, inc=1):
+    d[key] = d.get(key, 0) + inc
+
+
+def controlled_target(M, nq):
+    """If M (2^nq, Qiskit order) is a 2x2 on one gate qubit j controlled by all the others being 1,
+    return (j, U); else None (compiler.py:63-75)."""
+    full = (1 << nq) - 1
+    eye = np.eye(1 << nq)
+    for j in range(nq):
+        i1 = full
+        i0 = full & ~(1 << j)
+        sel = [i0, i1]
+        U = M[np.ix_(sel, sel)].copy()
+        rest = M.copy()
+        rest[np.ix_(sel, sel)] = I2
+        if np.allclose(rest, eye, atol=1e-12):
+            return j, U
+    return None
+
+
+def ops_2q(M, a, b, stats):
+    """4x4 gate on storage qubits (a, b), basis bit_a + 2*bit_b -> MUX2 ops (compiler.py:78-92):
+    diagonal -> one MUX2 on b selected by a; controlled-U -> one MUX2; otherwise the cosine-sine
+    decomposition into three MUX2 (block-diag on a | rotation on b | block-diag on a)."""
+    if np.allclose(M, np.diag(np.diag(M)), atol=1e-12):
+        d = np.diag(M)
+        return [Op(b, (a,), np.diag([d[0], d[2]]), np.diag([d[1], d[3]]))]
+    ct = controlled_target(M, 2)
+    if ct is not None:
+        j, U = ct
+        tgt, ctl = (a, b) if j == 0 else (b, a)
+        return [Op(tgt, (ctl,), I2, U)]
+    (u1, u2), theta, (v1h, v2h) = cossin(M, p=2, q=2, separate=True)
+    c, s = np.cos(theta), np.sin(theta)
+    R0 = np.array([[c[0], -s[0]], [s[0], c[0]]])
+    R1 = np.array([[c[1], -s[1]], [s[1], c[1]]])
+    stats.csd_2q += 1
+    return [Op(a, (b,), v1h, v2h), Op(b, (a,), R0, R1), Op(a, (b,), u1, u2)]
+
+
+def _lower(name, nq, params):
+    """Decomposition of a gate that cannot become MUX2 records directly, into gates that can.
+    Replaces the reference's ``transpile(..., basis_gates=["u", "cx"])`` (compiler.py:159-166); the
+    gate sequence differs from Qiskit's but implements the same unitary. Qubits are gate-local."""
+    if name == "cswap":
+        return [("cx", (2, 1), ()), ("ccx", (0, 1, 2), ()), ("cx", (2, 1), ())]
+    raise NotImplementedError(
+        f"gate {name!r} on {nq} qubits is neither a (multi-)controlled 2x2 nor wide-gate lowerable here")
+
+
+def circuit_to_ops(qc, stats, fuse_1q=True, max_width=None):
+    """Gates -> MUX2 ops (compiler.py:95-173). SWAPs become a relabelling (relab[l] = storage qubit of
+    logical qubit l); 1q gates on a qubit are multiplied together (complex128) until another gate
+    touches that qubit. Returns (ops, relab)."""
+    instrs = normalize(qc)
+    n = qc.num_qubits
+    relab = list(range(n))
+    ops = []
+    pending = {}
+
+    def flush(q):
+        if q in pending:
+            U = pending.pop(q)
+            ops.append(Op(q, (), U, U))
+
+    def emit(new_ops):
+        for op in new_ops:
+            for q in op.q:
+                flush(q)
+            ops.append(op)
+
+    def handle(name, qs, params, lowered):
+        if name in SKIP:
+            return
+        if not lowered:
+            stats.n_input_gates += 1
+        if name == "swap":
+            a, b = qs
+            relab[a], relab[b] = relab[b], relab[a]
+            stats.relabel += 1
+            return
+        st = [relab[q] for q in qs]
+        nq = len(qs)
+        if nq > 2 and name in MC_NAMES and (max_width is None or nq <= max_width):
+            if not lowered:
+                _count(stats.native, name)
+            U = mc_matrix(name, nq - 1, params)
+            emit([Op(st[-1], tuple(st[:-1]), I2, U, src=(name, qs))])
+            return
+        if nq > 2 and ((max_width is not None and nq > max_width) or nq > MAX_DENSE_QUBITS):
+            if not lowered:
+                _count(stats.native, name)
+            lower(name, qs, params)
+            return
+        M = gate_matrix(name, params)
+        if not lowered:
+            _count(stats.native, name)
+        if nq == 1:
+            s = st[0]
+            if fuse_1q and s in pending:
+                pending[s] = M @ pending[s]
+                stats.fused_1q += 1
+            elif fuse_1q:
+                pending[s] = M
+            else:
+                ops.append(Op(s, (), M, M))
+            return
+        if nq == 2:
+            emit(ops_2q(M, st[0], st[1], stats))
+            return
+        ct = controlled_target(M, nq)
+        if ct is not None:
+            j, U = ct
+            emit([Op(st[j], tuple(x for i, x in enumerate(st) if i != j), I2, U, src=(name, qs))])
+            return
+        lower(name, qs, params)
+
+    def lower(name, qs, params):
+        _count(stats.native, name, -1)
+        _count(stats.lowered, name)
+        for sub_name, sub_qs, sub_params in _lower(name, len(qs), params):
+            handle(sub_name, [qs[i] for i in sub_qs], sub_params, True)
+
+    for name, qs, params in instrs:
+        handle(name, list(qs), params, False)
+    for q in list(pending):
+        flush(q)
+    stats.n_ops = len(ops)
+    return ops, relab
+
+
+def pass_window(qubits, k, max_high=MAX_HIGH):
+    """Smallest m in 0..max_high such that at most m of `qubits` lie at or above k - m; returns
+    (m, sorted high qubits), or None when no m fits (compiler.py:176-183)."""
+    for m in range(max_high + 1):
+        hi = sorted(q for q in qubits if q >= k - m)
+        if len(hi) <= m:
+            return m, hi
+    return None
+
+
+def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=MAX_HIGH):
+    """Greedy pass packing with remap insertion (compiler.py:186-260).
+
+    Ops are taken in program order. An op joins the open pass while the pass's qubits still fit one tile
+    window (k - m low qubits plus m <= M high qubits) and the pass holds fewer than 64 ops. An op that
+    touches a bank qubit (>= L) or cannot fit any window closes the segment and emits a remap that brings
+    its qubits into the window, evicting the qubits whose next use is furthest away.
+    Returns (steps, l2p) with steps [("segment", [pass, ...]) | ("remap", perm)], a pass being a list of
+    (op, physical qubits)."""
+    l2p = list(l2p0) if l2p0 is not None else list(range(n))
+    k = min(k, L)
+    steps = []
+    seg = []
+    cur, cur_set = [], set()
+
+    def close_pass():
+        nonlocal cur, cur_set
+        if cur:
+            seg.append(cur)
+        cur, cur_set = [], set()
+
+    def close_segment():
+        close_pass()
+        if seg:
+            steps.append(("segment", list(seg)))
+            seg.clear()
+
+    def next_use(p, idx):
+        logical = l2p.index(p)
+        for j in range(idx, len(ops)):
+            if logical in ops[j].q:
+                return j - idx
+        return 10 ** 9
+
+    for idx, op in enumerate(ops):
+        phys = [l2p[q] for q in op.q]
+        if any(p >= L for p in phys) or pass_window(set(phys), k, M) is None:
+            low = k - M
+            assert len(phys) <= low + M, "op wider than the tile window"
+            by_far = lambda p: -next_use(p, idx)          # noqa: E731  furthest next use first
+            bank = [p for p in phys if p >= L]
+            high_local = [p for p in phys if low <= p < L]
+            hi_slots = sorted((p for p in range(max(k, L - 6), L) if p not in phys), key=by_far)
+            if bank and len(high_local) + len(bank) <= M and len(hi_slots) >= len(bank):
+                move, victims = bank, hi_slots[:len(bank)]
+            else:
+                keep = high_local[:M]
+                move = [p for p in phys if p >= low and p not in keep]
+                low_slots = sorted((p for p in range(low) if p not in phys), key=by_far)
+                high_slots = sorted((p for p in range(low, L) if p not in phys), key=by_far)
+                high_free = M - len(keep)
+                victims = []
+                for _ in move:
+                    if low_slots:
+                        victims.append(low_slots.pop(0))
+                    elif high_free > 0 and high_slots:
+                        victims.append(high_slots.pop(0))
+                        high_free -= 1
+                    else:
+                        raise RuntimeError("cannot fit op into tile window")
+            close_segment()
+            perm = list(range(n))
+            for a, b in zip(move, victims):
+                perm[a], perm[b] = b, a
+            steps.append(("remap", perm))
+            stats.n_remaps += 1
+            new_of_old = {old: new for new, old in enumerate(perm)}
+            l2p = [new_of_old[p] for p in l2p]
+            phys = [l2p[q] for q in op.q]
+        grown = cur_set | set(phys)
+        if (not tiling and cur) or len(cur) >= MAX_OPS_PER_PASS or pass_window(grown, k, M) is None:
+            close_pass()
+            grown = set(phys)
+        cur.append((op, phys))
+        cur_set = grown
+    close_segment()
+    return steps, l2p
+
+
+def encode_segment(passes, L, k, M=MAX_HIGH):
+    """QSV2 words of one segment (compiler.py:263-285). Matrices are rounded to complex64 here: this
+    is the single FP64 -> FP32 rounding point of the program."""
+    words = [MAGIC, L, len(passes), k, 0, 0, 0, 0]
+    for p in passes:
+        qubits = set(q for _, ph in p for q in ph)
+        m, hi = pass_window(qubits, k, M)
+        slots = hi + [0] * (4 - len(hi))
+        tile_of = {q: q for q in qubits if q < k - m}
+        for i, q in enumerate(hi):
+            tile_of[q] = k - m + i
+        words += [m, slots[0], slots[1], len(p), slots[2], slots[3], 0, 0]
+        for op, ph in p:
+            tq = [tile_of[q] for q in ph]
+            cmask = 0
+            for c in tq[1:]:
+                cmask |= 1 << c
+            f = np.zeros(16, dtype=np.float32)
+            for i, mat in enumerate((op.M0, op.M1)):
+                c64 = np.asarray(mat, dtype=np.complex64).reshape(-1)
+                f[8 * i:8 * i + 8:2] = c64.real
+                f[8 * i + 1:8 * i + 8:2] = c64.imag
+            words += [OP_MUX2, tq[0], cmask, 0, 0, 0, 0, 0] + list(f.view(np.int32))
+    arr = np.asarray(words, dtype=np.int64)
+    return (arr & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
+
+
+def compile_circuit(qc, L, k, fuse_1q=True, tiling=True, remap_policy="lru", initial_map=None,
+                    max_high=MAX_HIGH):
+    """Full pipeline (compiler.py:288-314). Returns (prog, final_map, stats); final_map[l] is the
+    physical position of logical qubit l after the program."""
+    k = min(k, L)
+    max_high = max(0, min(max_high, k - 3))      # sub-blocks of at least 2^3 amplitudes
+    stats = Stats()
+    ops, relab = circuit_to_ops(qc, stats, fuse_1q, max_width=k)
+    n = qc.num_qubits
+    steps, l2p_end = schedule(ops, n, L, k, stats, remap_policy, tiling, initial_map, max_high)
+    prog = []
+    if initial_map is not None and list(initial_map) != list(range(n)):
+        perm = [0] * n
+        for logical, p in enumerate(initial_map):
+            perm[p] = logical
+        prog.append(("remap", perm))
+    for kind, payload in steps:
+        if kind == "segment":
+            prog.append(("segment", encode_segment(payload, L, k, max_high)))
+            stats.n_segments += 1
+            stats.n_passes += len(payload)
+        else:
+            prog.append(("remap", payload))
+    final_map = [l2p_end[relab[q]] for q in range(n)]
+    return prog, final_map, stats

@@ -1,0 +1,152 @@
+"""Gate matrices in the Qiskit convention (complex128).
+
+For a gate applied to qubits (q0, q1, ...), basis index = bit(q0) + 2*bit(q1) + 4*bit(q2) ...
+(the little-endian order that Qiskit's ``Operator(gate).data`` uses, and that the reference compiler
+relies on in ``ops_2q``: "M: 4x4, basis bit_a + 2*bit_b", host/sv/compiler.py:79). Controlled gates
+put their controls first and the target last, as Qiskit does.
+"""
+import cmath
+import math
+
+import numpy as np
+
+I2 = np.eye(2, dtype=complex)
+X = np.array([[0, 1], [1, 0]], dtype=complex)
+Y = np.array([[0, -1j], [1j, 0]], dtype=complex)
+Z = np.diag([1, -1]).astype(complex)
+H = np.array([[1, 1], [1, -1]], dtype=complex) / math.sqrt(2)
+S = np.diag([1, 1j]).astype(complex)
+SDG = np.diag([1, -1j]).astype(complex)
+T = np.diag([1, cmath.exp(1j * math.pi / 4)]).astype(complex)
+TDG = np.diag([1, cmath.exp(-1j * math.pi / 4)]).astype(complex)
+SX = 0.5 * np.array([[1 + 1j, 1 - 1j], [1 - 1j, 1 + 1j]], dtype=complex)
+SXDG = 0.5 * np.array([[1 - 1j, 1 + 1j], [1 + 1j, 1 - 1j]], dtype=complex)
+
+
+def u3(theta, phi, lam):
+    c, s = math.cos(theta / 2), math.sin(theta / 2)
+    return np.array([[c, -cmath.exp(1j * lam) * s],
+                     [cmath.exp(1j * phi) * s, cmath.exp(1j * (phi + lam)) * c]], dtype=complex)
+
+
+def rx(th):
+    c, s = math.cos(th / 2), math.sin(th / 2)
+    return np.array([[c, -1j * s], [-1j * s, c]], dtype=complex)
+
+
+def ry(th):
+    c, s = math.cos(th / 2), math.sin(th / 2)
+    return np.array([[c, -s], [s, c]], dtype=complex)
+
+
+def rz(th):
+    return np.diag([cmath.exp(-0.5j * th), cmath.exp(0.5j * th)]).astype(complex)
+
+
+def phase(lam):
+    return np.diag([1, cmath.exp(1j * lam)]).astype(complex)
+
+
+def r_gate(theta, phi):
+    c, s = math.cos(theta / 2), math.sin(theta / 2)
+    return np.array([[c, -1j * cmath.exp(-1j * phi) * s],
+                     [-1j * cmath.exp(1j * phi) * s, c]], dtype=complex)
+
+
+def controlled(U, n_ctrl=1):
+    """Controls on gate qubits 0..n_ctrl-1, target on the last gate qubit."""
+    nq = n_ctrl + 1
+    d = 1 << nq
+    M = np.eye(d, dtype=complex)
+    on = (1 << n_ctrl) - 1
+    i0, i1 = on, on | (1 << n_ctrl)
+    M[np.ix_([i0, i1], [i0, i1])] = U
+    return M
+
+
+def _kron_le(*ops):
+    """Little-endian tensor product: ops[0] acts on gate qubit 0 (least significant)."""
+    out = np.array([[1]], dtype=complex)
+    for op in ops:
+        out = np.kron(op, out)
+    return out
+
+
+def _expm_herm(G, th):
+    """exp(-i th/2 G) for G with G @ G = I."""
+    return math.cos(th / 2) * np.eye(G.shape[0]) - 1j * math.sin(th / 2) * G
+
+
+SWAP = np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, 1, 0, 0], [0, 0, 0, 1]], dtype=complex)
+ISWAP = np.array([[1, 0, 0, 0], [0, 0, 1j, 0], [0, 1j, 0, 0], [0, 0, 0, 1]], dtype=complex)
+ECR = np.array([[0, 1, 0, 1j], [1, 0, -1j, 0], [0, 1j, 0, 1], [-1j, 0, 1, 0]], dtype=complex) / math.sqrt(2)
+DCX = np.array([[1, 0, 0, 0], [0, 0, 0, 1], [0, 1, 0, 0], [0, 0, 1, 0]], dtype=complex)
+
+
+def cswap():
+    M = np.eye(8, dtype=complex)
+    # control = gate qubit 0; swap gate qubits 1 and 2 when it is set: |c=1,a=1,b=0> <-> |c=1,a=0,b=1>
+    i, j = 0b011, 0b101
+    M[[i, j]] = M[[j, i]]
+    return M
+
+
+def xx_plus_yy(theta, beta=0.0):
+    c, s = math.cos(theta / 2), math.sin(theta / 2)
+    M = np.eye(4, dtype=complex)
+    M[1, 1] = c
+    M[2, 2] = c
+    M[1, 2] = -1j * s * cmath.exp(-1j * beta)
+    M[2, 1] = -1j * s * cmath.exp(1j * beta)
+    return M
+
+
+# name -> (number of qubits, number of params, matrix builder)
+_ONE = {
+    "id": (0, lambda: I2), "x": (0, lambda: X), "y": (0, lambda: Y), "z": (0, lambda: Z),
+    "h": (0, lambda: H), "s": (0, lambda: S), "sdg": (0, lambda: SDG), "t": (0, lambda: T),
+    "tdg": (0, lambda: TDG), "sx": (0, lambda: SX), "sxdg": (0, lambda: SXDG),
+    "rx": (1, rx), "ry": (1, ry), "rz": (1, rz), "p": (1, phase), "u1": (1, phase),
+    "u": (3, u3), "u3": (3, u3), "u2": (2, lambda phi, lam: u3(math.pi / 2, phi, lam)),
+    "r": (2, r_gate),
+}
+
+
+def gate_matrix(name, params=()):
+    """Dense Qiskit-convention matrix of a named gate (1q, 2q and the supported multi-qubit gates)."""
+    p = [float(x) for x in params]
+    if name in _ONE:
+        npar, f = _ONE[name]
+        return f(*p[:npar]) if npar else f()
+    two = {
+        "cx": lambda: controlled(X), "cy": lambda: controlled(Y), "cz": lambda: controlled(Z),
+        "ch": lambda: controlled(H), "csx": lambda: controlled(SX), "cs": lambda: controlled(S),
+        "csdg": lambda: controlled(SDG),
+        "cp": lambda: controlled(phase(p[0])), "cu1": lambda: controlled(phase(p[0])),
+        "crx": lambda: controlled(rx(p[0])), "cry": lambda: controlled(ry(p[0])),
+        "crz": lambda: controlled(rz(p[0])),
+        "cu": lambda: controlled(cmath.exp(1j * p[3]) * u3(p[0], p[1], p[2])),
+        "cu3": lambda: controlled(u3(p[0], p[1], p[2])),
+        "swap": lambda: SWAP, "iswap": lambda: ISWAP, "ecr": lambda: ECR, "dcx": lambda: DCX,
+        "rxx": lambda: _expm_herm(_kron_le(X, X), p[0]),
+        "ryy": lambda: _expm_herm(_kron_le(Y, Y), p[0]),
+        "rzz": lambda: _expm_herm(_kron_le(Z, Z), p[0]),
+        "rzx": lambda: _expm_herm(_kron_le(Z, X), p[0]),
+        "xx_plus_yy": lambda: xx_plus_yy(p[0], p[1] if len(p) > 1 else 0.0),
+        "ccx": lambda: controlled(X, 2), "ccz": lambda: controlled(Z, 2),
+        "cswap": cswap, "c3x": lambda: controlled(X, 3), "c4x": lambda: controlled(X, 4),
+    }
+    if name in two:
+        return two[name]()
+    raise KeyError(f"no matrix for gate {name!r}")
+
+
+def mc_matrix(name, n_ctrl, params=()):
+    """Target matrix U of a multi-controlled gate (controls all-ones select U)."""
+    if name in ("mcx", "ccx", "c3x", "c4x", "mcx_gray", "mcx_recursive"):
+        return X
+    if name == "ccz":
+        return Z
+    if name in ("mcp", "mcphase"):
+        return phase(float(params[0]))
+    raise KeyError(name)
