@@ -1,0 +1,295 @@
+"""Benchmark: QSV2 pass-sweep bandwidth of the 30-qubit random-layer circuit on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: random-layer circuit, 30 qubits, depth 24, seed 1 (U3 with angles uniform in [0, 2pi) on every
+qubit, CX brickwork), complex64 (8 GiB state), compiled to QSV2 by the reference scheduler (k = 12,
+M = 4). One step = the whole program (every sweep of every segment) over the resident state; the state
+(8 GiB) is far larger than L2 (126 MB), so no flush is needed between steps.
+
+value: algorithmic bytes (16 B per amplitude per sweep: one complex64 read + one write) over device time
+(CUDA events on the launch stream, max over ranks). e2e: the same metric through the public API
+(SVRuntime.run with host-side circuit, compile, instruction upload, device execution, device sampling
+and the read-back of 1024 sampled indices), per step.
+
+--gpus N > 1 runs N independent replicas (one process per GPU under torchrun): the path does not
+partition one state across GPUs, so there is no collective; value is the aggregate.
+--impl reference times the reference's own CPU implementation of the path (the numpy golden model,
+host/sv/model.py, restated in oracle/golden_model.py) on a bounded sample of the same workload, with
+every host core (spawned worker processes over disjoint tiles).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "u55c-statevector-30q_b200")
+METRIC = "30q pass sweep GB/s (random-layer d24)"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _package():
+    import importlib.util
+    if "qsv_b200" in sys.modules:
+        return sys.modules["qsv_b200"]
+    spec = importlib.util.spec_from_file_location("qsv_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["qsv_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(pkg, n, depth, seed, k=12, max_high=4):
+    gen = pkg.generators
+    qc = gen.random_layer(n, depth, seed)
+    prog, fmap, stats = pkg.compile_circuit(qc, n, k, max_high=max_high)
+    return qc, prog, fmap, stats
+
+
+# ------------------------------------------------------------------ CPU baseline (golden model)
+def _cpu_worker(args):
+    seg, n, tiles, npass = args
+    sys.path.insert(0, ROOT)
+    from oracle import golden_model as gm
+    state = np.zeros(1 << n, dtype=np.complex64)     # lazily mapped: only the sampled tiles are touched
+    state[0] = 1
+    t0 = time.perf_counter()
+    moved = gm.run_segment_tiles(state, seg, tiles, npass)
+    return moved, time.perf_counter() - t0
+
+
+def cpu_sample(seg, n, n_tiles_total, seconds=12.0, workers=None):
+    """Golden model on a bounded sample of the workload: the first passes of the 30-qubit segment over a
+    spread of tiles, in parallel worker processes. Returns (GB/s, cores, description)."""
+    import multiprocessing as mp
+    workers = workers or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    # calibrate on one worker: tiles per second
+    probe = np.arange(0, n_tiles_total, max(1, n_tiles_total // 16), dtype=np.int64)[:16]
+    with ctx.Pool(1) as p:
+        moved, dt = p.map(_cpu_worker, [(seg, n, probe, 2)])[0]
+    rate = len(probe) / max(dt, 1e-6)
+    per_worker = max(16, int(rate * seconds / 2))
+    stride = max(1, n_tiles_total // (per_worker * workers))
+    jobs = []
+    for w in range(workers):
+        t = (np.arange(per_worker, dtype=np.int64) * workers + w) * stride % n_tiles_total
+        jobs.append((seg, n, t, 2))
+    t0 = time.perf_counter()
+    with ctx.Pool(workers) as p:
+        res = p.map(_cpu_worker, jobs)
+    wall = time.perf_counter() - t0
+    moved = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    desc = (f"golden model (numpy port of host/sv/model.py), first 2 passes of the 30-qubit segment on "
+            f"{per_worker * workers} of {n_tiles_total} tiles ({workers} processes), bytes = 16 B x amplitudes "
+            f"touched; GB/s over the slowest worker's time")
+    return moved / busy / 1e9, workers, desc, wall
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=24)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pkg = _package()
+    qc, prog, fmap, stats = workload(pkg, a.n, a.depth, a.seed)
+    segs = [p for kind, p in prog if kind == "segment"]
+    cfg = {"workload": f"random_layer n={a.n} depth={a.depth} seed={a.seed}, complex64 ({8 << a.n >> 30} GiB "
+                       f"state), QSV2 k=12 M=4 from the reference scheduler",
+           "n_qubits": a.n, "depth": a.depth, "qsv2_passes": stats.n_passes, "ops": stats.n_ops,
+           "l2": "inputs larger than L2 (8 GiB state vs 126 MB), no flush", "parallelism": f"replicas x{a.gpus}"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        tiles_total = 1 << (a.n - 12)
+        vals = []
+        for s in range(a.warmup + a.steps):
+            gbs, cores, desc, wall = cpu_sample(segs[0], a.n, tiles_total, seconds=6.0)
+            if s >= a.warmup:
+                vals.append(gbs)
+        v = statistics.median(vals)
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": a.gpus,
+                          "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "c64 (fp32)", "data": "synthetic (seeded circuit)",
+                          "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": "port", "sample": desc},
+                          "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    engine.load()
+    sweeps = sum(len(engine.plan_segment(s, a.n)) for s in segs)
+    cfg["sweeps"] = sweeps
+    stream = torch.cuda.current_stream(dev)
+    state = engine.new_state(a.n, device=dev)
+
+    def step():
+        for s in segs:
+            engine.run_segment(state, s, stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    engine.take_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    launches = engine.take_launch_count()
+    sec = e0.elapsed_time(e1) / 1e3
+    if dist:
+        t = torch.tensor([sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        dist.barrier()
+    bytes_per_sweep = 16 << a.n
+    total_bytes = bytes_per_sweep * sweeps * a.steps * world
+    value = total_bytes / sec / 1e9
+    per_launch = sec / (sweeps * a.steps)
+    peak, peak_kind = _peaks()
+    achieved = bytes_per_sweep / per_launch / 1e9
+
+    # end to end through the public API (host circuit in, sampled counts out)
+    from qsv_b200.runtime import SVRuntime
+    rt = SVRuntime(device=dev)
+    rt.run(qc, shots=1024, return_state=False, seed=0)
+    torch.cuda.synchronize(dev)
+    e2e_t = []
+    for i in range(a.e2e_steps):
+        t0 = time.perf_counter()
+        r = rt.run(qc, shots=1024, return_state=False, seed=i)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_sec = max(statistics.median(e2e_t), 1e-9)
+    if dist:
+        t = torch.tensor([e2e_sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_sec = float(t.item())
+    seg_bytes = sum(np.asarray(s).nbytes for s in segs)
+    e2e = {"value": bytes_per_sweep * sweeps * world / e2e_sec / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": seg_bytes + 8 * 1024, "d2h_bytes_per_step": 8 * 1024,
+           "ms_per_step": e2e_sec * 1e3, "T_kernel_s": r["timing"]["T_kernel"], "T_compile_s": r["timing"]["T_compile"]}
+
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu:
+            gbs, cores, desc, wall = cpu_sample(segs[0], a.n, 1 << (a.n - 12), seconds=10.0)
+            cpu = {"value": gbs, "unit": "GB/s", "cores": cores, "kind": "port", "sample": desc}
+        out = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": sec / a.steps * 1e3, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 arithmetic)",
+               "data": "synthetic (seeded random-layer circuit)", "config": cfg,
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                            "kernel": "qsv::dev::sweep_kernel<13,4,3,3>",
+                            "algorithmic_bytes_per_launch": bytes_per_sweep},
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

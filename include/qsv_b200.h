@@ -1,0 +1,111 @@
+/*
+ * qsv_b200.h -- C ABI of libqsv_b200.so, the B200 (sm_100a) QSV2 statevector engine.
+ *
+ * The entry points replace the reference's device calls one for one (paths are within the reference
+ * project nasir26/u55c-statevector-30q):
+ *   qsv_run_segment   <- sv_engine(st, ins_off)            kernels/sv/sv_engine.cpp:302-331,
+ *                        launched per slice at host/sv/runtime.py:227-233 (_run_segment)
+ *   qsv_remap         <- sv_swap(a, b, offa, offb, nw)     kernels/sv/sv_swap.cpp:10-39 and the host
+ *                        exchange of host/sv/runtime.py:235-284 (_swap_bank_local/_swap_local_local/_remap)
+ *   qsv_zero_state    <- _zero_segment/_init_zero_state    host/sv/runtime.py:205-217
+ *   qsv_chunk_probs_f64, qsv_sample_f64
+ *                     <- sample_slices (host Born sampling) host/sv/runtime.py:47-80, moved on device
+ *   qsv_reduce_f64    <- the norm check of tests/functional_suite.py:92-94 and the per-qubit <Z>
+ *                        outputs of the batched workload; no device counterpart in the reference
+ *   qsv_plan_segment  <- model.decode (host/sv/model.py:7-22): exposes how a segment is executed
+ *
+ * Conventions: every function returns QSV_OK (0) or a negative QSV_ERR_* code and never throws;
+ * qsv_last_error() gives a message for the calling thread's last failure. Device pointers are plain
+ * CUDA device addresses (the Python runtime passes PyTorch tensor storage); `stream` is a cudaStream_t
+ * (NULL = legacy default stream). Calls are asynchronous on `stream` unless stated otherwise; the host
+ * arrays they read (segment words, permutations) may be reused as soon as the call returns. The library
+ * allocates no device memory on these paths: scratch is passed in by the caller.
+ * State layout: 2^n amplitudes, little-endian qubit order (qubit q = index bit q), complex64 as
+ * interleaved float32 (re, im) -- the numpy complex64 layout the reference uses (sv_engine.cpp:4-5).
+ */
+#ifndef QSV_B200_H
+#define QSV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define QSV_API __attribute__((visibility("default")))
+#else
+#define QSV_API
+#endif
+
+#define QSV_OK 0
+#define QSV_ERR_INVALID_ARG (-1)   /* null pointer, size out of range, bad permutation */
+#define QSV_ERR_BAD_STREAM (-2)    /* malformed QSV2 segment (magic, header, record bounds) */
+#define QSV_ERR_UNSUPPORTED (-3)   /* well-formed but beyond this engine (window wider than 13 qubits) */
+#define QSV_ERR_CUDA (-4)          /* a CUDA runtime call failed; see qsv_last_error() */
+#define QSV_ERR_DEVICE (-5)        /* a kernel reported a fault through the device status word */
+#define QSV_ERR_SCRATCH (-6)       /* caller-provided scratch smaller than required */
+
+#define QSV_C64 0                  /* complex64 amplitudes (QSV2, fp32 matrices) */
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+QSV_API int qsv_version(void);
+
+/* Message of the calling thread's last error ("" if none). */
+QSV_API const char *qsv_last_error(void);
+
+/* Execute one QSV2 segment (every pass, in order) on the device state in place.
+ * Replaces sv_engine (kernels/sv/sv_engine.cpp:302); `seg` is the host copy of the words the reference
+ * runtime uploads behind each slice (host/sv/runtime.py:218-225). The segment's L must equal n.
+ * Consecutive passes are merged into sweeps whose qubit window fits the engine's 13-qubit tile; the
+ * result equals pass-by-pass execution value for value. n in [10, 34]. */
+QSV_API int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int dtype, void *stream);
+
+/* Qubit permutation, out of place: dst[y] = src[x] with bit j of y = bit perm[j] of x
+ * (perm[new_phys] = old_phys, host/sv/model.py:74-78). Replaces the sv_swap exchange and the host
+ * remaps of host/sv/runtime.py:235-284 with one in-HBM sweep. src and dst must not overlap. */
+QSV_API int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, void *stream);
+
+/* |0...0>: zero the state and set amplitude 0 to 1 (host/sv/runtime.py:205-217). */
+QSV_API int qsv_zero_state(void *state, int n, int dtype, void *stream);
+
+/* Bytes of scratch the reductions and the sampler need for a 2^n state. */
+QSV_API size_t qsv_reduce_scratch_bytes(int n);
+
+/* FP64 reductions over |a_i|^2: out_dev[0] = sum |a_i|^2, out_dev[1 + q] = <Z_q> = sum (1 - 2 bit_q(i))
+ * |a_i|^2 for q < n (n + 1 doubles, device memory). */
+QSV_API int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *scratch, size_t scratch_bytes,
+                   void *stream);
+
+/* Probability of each chunk of 2^chunk_bits consecutive amplitudes, FP64 (2^(n - chunk_bits) doubles).
+ * The first level of the reference's hierarchical sampler (host/sv/runtime.py:59-63). */
+QSV_API int qsv_chunk_probs_f64(const void *state, int n, int dtype, int chunk_bits, double *out_dev, void *stream);
+
+/* Born-rule sampling on the device: for each of `shots` uniforms u in [0, 1) (device array), the
+ * physical index i with cdf(i-1) <= u * total < cdf(i), cdf in FP64 over chunk sums then within the
+ * chosen chunk (the search of host/sv/runtime.py:64-75). Writes int64 indices to out_dev. */
+QSV_API int qsv_sample_f64(const void *state, int n, int dtype, const double *uniforms_dev, int shots, int64_t *out_dev,
+                   void *scratch, size_t scratch_bytes, void *stream);
+
+/* Host-side decode of a segment into the sweep plan the engine launches, for inspection and tests.
+ * Writes at most `cap` int32 words to `out` (layout in csrc/qsv_plan.h, qsv_plan_serialize) and returns
+ * the number of words of the full plan, or a negative error code. Pure host code, no device work. */
+QSV_API int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap);
+
+/* Read and clear the device status word that kernels set when a bounded wait gives up (0 = clean).
+ * Synchronous. */
+QSV_API int qsv_device_status(int *status);
+
+/* Number of kernel launches this thread issued through this library since the last call (and reset
+ * the count). No reference counterpart: launch accounting for the benchmark. */
+QSV_API long long qsv_take_launch_count(void);
+
+/* Tuning knob (no reference counterpart): merged sweeps keep sub-blocks of at least 2^lo amplitudes
+ * contiguous (lo in [3, 13]; default 4 = 128 bytes). Larger values merge fewer passes. Process-wide. */
+QSV_API int qsv_set_lo_merge(int lo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QSV_B200_H */

@@ -110,3 +110,31 @@ def run_program(prog, n, P, final_map, state=None):
         else:
             state = remap(state, n, payload)
     return unpermute(state, n, final_map)
+
+
+def run_segment_tiles(state, seg, tiles, n_passes=None):
+    """The golden model's run_segment restricted to the given tile numbers of every pass (same tile
+    addressing and arithmetic as tile_index_map / apply_op_tile); a bounded sample of a full segment for
+    timing the CPU baseline at sizes where the whole segment would take hours. Returns the amplitudes
+    read + written (bytes)."""
+    L, k, passes = decode(seg)
+    tiles = np.asarray(tiles, dtype=np.int64)
+    moved = 0
+    for m, highs, ops in passes[:n_passes]:
+        low = k - m
+        taken = set(range(low)) | set(highs[:m])
+        free = [b for b in range(L) if b not in taken]
+        j = np.arange(1 << k, dtype=np.int64)
+        within = j & ((1 << low) - 1)
+        for i, h in enumerate(highs[:m]):
+            within |= ((j >> (low + i)) & 1) << h
+        base = np.zeros_like(tiles)
+        for i, b in enumerate(free):
+            base |= ((tiles >> i) & 1) << b
+        idx = base[:, None] | within[None, :]
+        T = state[idx]
+        for code, t, cm, M0, M1 in ops:
+            apply_op_tile(T, code, t, cm, M0, M1)
+        state[idx] = T
+        moved += T.size * 16
+    return moved

@@ -1,0 +1,55 @@
+"""Builds libqsv_b200.so in place with nvcc for sm_100a (cross-compiles on a machine without a GPU).
+
+    python u55c-statevector-30q_b200/build.py [--force] [--verbose]
+
+The library links the CUDA runtime statically, so it does not depend on which libcudart the host
+process (PyTorch) loaded; both talk to the driver's primary context.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libqsv_b200.so")
+SOURCES = ["qsv_capi.cu", "qsv_sweep.cu", "qsv_aux.cu", "qsv_planner.cpp"]
+HEADERS = ["qsv_plan.h", "qsv_planner.h", "qsv_device.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "qsv_b200.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force=False, verbose=False):
+    if not force and not stale():
+        return LIB
+    cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo", *ARCH, "--shared", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+           "-cudart", "static", "--expt-relaxed-constexpr", "-o", LIB + ".tmp"]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if verbose:
+        sys.stderr.write(r.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
+    print(LIB)

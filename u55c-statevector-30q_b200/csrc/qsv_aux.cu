@@ -1,0 +1,330 @@
+// qsv_aux.cu -- the remap (qubit permutation) kernel, |0..0> init, FP64 reductions and the Born sampler.
+//
+// remap: replaces the reference's exchange path -- sv_swap (kernels/sv/sv_swap.cpp:10-39) for
+// bank<->local transpositions and the host permutes of host/sv/runtime.py:261-268 -- with one in-HBM
+// sweep for an arbitrary bit permutation perm[new] = old (host/sv/model.py:74-78). Each CTA moves tiles
+// of 2^10 amplitudes that are contiguous in 32-amplitude runs on both sides: the tile holds source bits
+// 0..4 (coalesced reads) and the source bits that land on destination bits 0..4 (coalesced writes),
+// padded with the lowest remaining source bits; the transpose happens in shared memory.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qsv_device.cuh"
+
+namespace qsv {
+namespace dev {
+
+#define REMAP_TB 10                 // tile bits
+#define REMAP_RUN 5                 // contiguous run bits on each side
+#define REMAP_THREADS 256
+
+struct RemapParams {
+    int n;
+    int nfree;
+    uint8_t ubits[REMAP_TB];        // source bits of the tile, ascending (tile position bit i <-> ubits[i])
+    uint8_t fx[40];                 // free source bits, ascending
+    uint8_t fy[40];                 // destination position of free source bit fx[i]
+    uint8_t ypos[REMAP_TB];         // destination position of tile source bit ubits[i]
+};
+
+__global__ void __launch_bounds__(REMAP_THREADS)
+    remap_kernel(const float2 *__restrict__ src, float2 *__restrict__ dst, const __grid_constant__ RemapParams P) {
+    constexpr int TS = 1 << REMAP_TB;
+    __shared__ float2 tile[TS];
+    __shared__ uint64_t rd_off[TS];
+    __shared__ uint64_t wr_off[TS];
+    __shared__ uint16_t wr_pos[TS];
+    // destination-side enumeration: k's bits walk the destination positions of the tile bits, ascending,
+    // so k's low bits are destination bits 0..4 (coalesced writes)
+    uint8_t order[REMAP_TB];        // order[q] = tile bit whose destination position is the q-th smallest
+    {
+        bool used[REMAP_TB] = {false};
+        for (int q = 0; q < REMAP_TB; q++) {
+            int best = -1;
+            for (int i = 0; i < REMAP_TB; i++)
+                if (!used[i] && (best < 0 || P.ypos[i] < P.ypos[best])) best = i;
+            used[best] = true;
+            order[q] = (uint8_t)best;
+        }
+    }
+    for (int j = threadIdx.x; j < TS; j += REMAP_THREADS) {
+        uint64_t o = 0;
+        for (int i = 0; i < REMAP_TB; i++)
+            if ((j >> i) & 1) o |= 1ull << P.ubits[i];
+        rd_off[j] = o;
+        uint64_t w = 0;
+        uint32_t pos = 0;
+        for (int q = 0; q < REMAP_TB; q++)
+            if ((j >> q) & 1) {
+                w |= 1ull << P.ypos[order[q]];
+                pos |= 1u << order[q];
+            }
+        wr_off[j] = w;
+        wr_pos[j] = (uint16_t)pos;
+    }
+    __syncthreads();
+    const int64_t ntiles = 1ll << P.nfree;
+    for (int64_t T = blockIdx.x; T < ntiles; T += gridDim.x) {
+        uint64_t xb = 0, yb = 0;
+        for (int i = 0; i < P.nfree; i++)
+            if ((T >> i) & 1) {
+                xb |= 1ull << P.fx[i];
+                yb |= 1ull << P.fy[i];
+            }
+        for (int j = threadIdx.x; j < TS; j += REMAP_THREADS) tile[j] = src[xb | rd_off[j]];
+        __syncthreads();
+        for (int k = threadIdx.x; k < TS; k += REMAP_THREADS) dst[yb | wr_off[k]] = tile[wr_pos[k]];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- |0...0>
+__global__ void set_amp0_kernel(float2 *state) { state[0] = make_float2(1.0f, 0.0f); }
+
+// ---------------------------------------------------------------- FP64 reductions
+// Block b covers amplitudes [b << B, (b+1) << B). Thread t visits i = (b << B) + t + 256 * it. The
+// per-block result is 1 + B doubles: the block total and, for each bit q < B of the index, the sum of
+// |a_i|^2 over the block's i with bit q set. Fixed summation order (deterministic).
+#define RED_THREADS 256
+__global__ void __launch_bounds__(RED_THREADS)
+    reduce_block_kernel(const float2 *__restrict__ state, int B, double *__restrict__ partials) {
+    __shared__ double s_tot[RED_THREADS];
+    __shared__ double s_bits[RED_THREADS][17];
+    const int t = threadIdx.x;
+    const int64_t base = (int64_t)blockIdx.x << B;
+    const int niter = 1 << (B - 8);
+    double tot = 0.0;
+    double hb[17];                  // bits 8..B-1 of i (from it)
+#pragma unroll
+    for (int q = 0; q < 17; q++) hb[q] = 0.0;
+    // it = (g << 4) | k: the 16 values of k are summed per bit in registers, group totals feed the
+    // bits above
+    const int ng = niter >= 16 ? niter >> 4 : 1;
+    const int gk = niter >= 16 ? 16 : niter;
+    for (int g = 0; g < ng; g++) {
+        double u[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            u[k] = 0.0;
+            if (k < gk) {
+                const float2 a = state[base + t + ((int64_t)((g << 4) | k) << 8)];
+                u[k] = (double)a.x * a.x + (double)a.y * a.y;
+            }
+        }
+        double gt = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) gt += u[k];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 16; k++)
+                if ((k >> q) & 1) s += u[k];
+            hb[q] += s;
+        }
+        for (int q = 4; q < B - 8; q++)
+            if ((g >> (q - 4)) & 1) hb[q] += gt;
+        tot += gt;
+    }
+    s_tot[t] = tot;
+    for (int q = 0; q < 17; q++) s_bits[t][q] = hb[q];
+    __syncthreads();
+    double *out = partials + (int64_t)blockIdx.x * (B + 1);
+    if (t == 0) {
+        double s = 0.0;
+        for (int i = 0; i < RED_THREADS; i++) s += s_tot[i];
+        out[0] = s;
+    } else if (t <= B) {
+        const int q = t - 1;        // index bit q
+        double s = 0.0;
+        if (q < 8) {
+            for (int i = 0; i < RED_THREADS; i++)
+                if ((i >> q) & 1) s += s_tot[i];
+        } else {
+            for (int i = 0; i < RED_THREADS; i++) s += s_bits[i][q - 8];
+        }
+        out[1 + q] = s;
+    }
+}
+
+// out[0] = total, out[1 + q] = total - 2 * (sum over i with bit q set)
+__global__ void reduce_final_kernel(const double *__restrict__ partials, int nblocks, int B, int n,
+                                    double *__restrict__ out) {
+    const int t = threadIdx.x;
+    if (t > n) return;
+    double tot = 0.0, s = 0.0;
+    for (int b = 0; b < nblocks; b++) {
+        const double *p = partials + (int64_t)b * (B + 1);
+        tot += p[0];
+        if (t >= 1) {
+            const int q = t - 1;
+            if (q < B) s += p[1 + q];
+            else if ((b >> (q - B)) & 1) s += p[0];
+        }
+    }
+    if (t == 0) out[0] = tot;
+    else out[t] = tot - 2.0 * s;
+}
+
+// chunk probabilities: one block per chunk of 2^cb amplitudes
+__global__ void __launch_bounds__(RED_THREADS)
+    chunk_probs_kernel(const float2 *__restrict__ state, int cb, double *__restrict__ out) {
+    __shared__ double s[RED_THREADS];
+    const int64_t base = (int64_t)blockIdx.x << cb;
+    const int len = 1 << cb;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < len; i += RED_THREADS) {
+        const float2 a = state[base + i];
+        acc += (double)a.x * a.x + (double)a.y * a.y;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+// inclusive prefix sum of nc doubles in one block (sequential per thread slice, fixed order)
+__global__ void scan_kernel(double *__restrict__ v, int64_t nc) {
+    __shared__ double part[1024];
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int64_t per = (nc + nt - 1) / nt;
+    const int64_t b = t * per, e = b + per < nc ? b + per : nc;
+    double s = 0.0;
+    for (int64_t i = b; i < e; i++) s += v[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        double run = 0.0;
+        for (int i = 0; i < nt; i++) {
+            const double x = part[i];
+            part[i] = run;
+            run += x;
+        }
+    }
+    __syncthreads();
+    double run = part[t];
+    for (int64_t i = b; i < e; i++) {
+        run += v[i];
+        v[i] = run;
+    }
+}
+
+// one thread per shot: chunk by binary search on the FP64 chunk cdf, then a linear FP64 scan inside
+// the chunk (first index whose running sum exceeds the remainder, clipped to the chunk)
+__global__ void sample_kernel(const float2 *__restrict__ state, int cb, const double *__restrict__ cdf, int64_t nc,
+                              const double *__restrict__ uni, int shots, int64_t *__restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= shots) return;
+    const double total = cdf[nc - 1];
+    const double x = uni[s] * total;
+    int64_t lo = 0, hi = nc;        // first c with cdf[c] > x
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (cdf[mid] > x) hi = mid;
+        else lo = mid + 1;
+    }
+    int64_t c = lo < nc ? lo : nc - 1;
+    const double rem = x - (c > 0 ? cdf[c - 1] : 0.0);
+    const int len = 1 << cb;
+    const float2 *p = state + (c << cb);
+    double run = 0.0;
+    int j = 0;
+    for (; j < len; j++) {
+        const float2 a = p[j];
+        run += (double)a.x * a.x + (double)a.y * a.y;
+        if (run > rem) break;
+    }
+    if (j >= len) j = len - 1;
+    out[s] = (c << cb) + j;
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------- host launchers
+cudaError_t launch_remap(const float2 *src, float2 *dst, int n, const int32_t *perm, int nsm, cudaStream_t stream) {
+    dev::RemapParams P;
+    memset(&P, 0, sizeof(P));
+    P.n = n;
+    int inv[64];
+    for (int j = 0; j < n; j++) inv[perm[j]] = j;          // source bit perm[j] -> destination bit j
+    bool in_tile[64] = {false};
+    int cnt = 0;
+    for (int b = 0; b < REMAP_RUN; b++) { in_tile[b] = true; cnt++; }
+    for (int j = 0; j < REMAP_RUN; j++)
+        if (!in_tile[perm[j]]) { in_tile[perm[j]] = true; cnt++; }
+    for (int b = 0; b < n && cnt < REMAP_TB; b++)
+        if (!in_tile[b]) { in_tile[b] = true; cnt++; }
+    int nu = 0, nf = 0;
+    for (int b = 0; b < n; b++) {
+        if (in_tile[b]) {
+            P.ubits[nu] = (uint8_t)b;
+            P.ypos[nu] = (uint8_t)inv[b];
+            nu++;
+        } else {
+            P.fx[nf] = (uint8_t)b;
+            P.fy[nf] = (uint8_t)inv[b];
+            nf++;
+        }
+    }
+    P.nfree = nf;
+    const int64_t ntiles = 1ll << nf;
+    int64_t grid = (int64_t)nsm * 8;
+    if (grid > ntiles) grid = ntiles;
+    dev::remap_kernel<<<(unsigned)grid, REMAP_THREADS, 0, stream>>>(src, dst, P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_amp0(float2 *state, cudaStream_t stream) {
+    dev::set_amp0_kernel<<<1, 1, 0, stream>>>(state);
+    return cudaGetLastError();
+}
+
+int reduce_bits(int n) {
+    int B = n - 10;
+    if (B < 13) B = 13;
+    if (B > n) B = n;
+    if (B > 25) B = 25;
+    return B;
+}
+
+size_t reduce_scratch_bytes(int n, int chunk_bits) {
+    const int B = reduce_bits(n);
+    const size_t red = ((size_t)1 << (n - B)) * (B + 1) * sizeof(double);
+    const size_t smp = ((size_t)1 << (n - chunk_bits)) * sizeof(double);
+    return red > smp ? red : smp;
+}
+
+cudaError_t launch_reduce(const float2 *state, int n, double *out, void *scratch, cudaStream_t stream) {
+    const int B = reduce_bits(n);
+    const int nblocks = 1 << (n - B);
+    double *partials = (double *)scratch;
+    dev::reduce_block_kernel<<<nblocks, RED_THREADS, 0, stream>>>(state, B, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dev::reduce_final_kernel<<<1, 64, 0, stream>>>(partials, nblocks, B, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_chunk_probs(const float2 *state, int n, int cb, double *out, cudaStream_t stream) {
+    dev::chunk_probs_kernel<<<(unsigned)(1ll << (n - cb)), RED_THREADS, 0, stream>>>(state, cb, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni, int shots, int64_t *out,
+                          void *scratch, cudaStream_t stream) {
+    double *cdf = (double *)scratch;
+    const int64_t nc = 1ll << (n - cb);
+    dev::chunk_probs_kernel<<<(unsigned)nc, RED_THREADS, 0, stream>>>(state, cb, cdf);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dev::scan_kernel<<<1, 1024, 0, stream>>>(cdf, nc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (shots > 0) dev::sample_kernel<<<(shots + 127) / 128, 128, 0, stream>>>(state, cb, cdf, nc, uni, shots, out);
+    return cudaGetLastError();
+}
+
+}  // namespace qsv

@@ -1,0 +1,184 @@
+// qsv_capi.cu -- the extern "C" boundary of libqsv_b200.so (declared in include/qsv_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qsv_b200.h"
+#include "qsv_planner.h"
+
+namespace qsv {
+cudaError_t launch_sweep(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream);
+cudaError_t launch_remap(const float2 *src, float2 *dst, int n, const int32_t *perm, int nsm, cudaStream_t stream);
+cudaError_t launch_set_amp0(float2 *state, cudaStream_t stream);
+cudaError_t launch_reduce(const float2 *state, int n, double *out, void *scratch, cudaStream_t stream);
+cudaError_t launch_chunk_probs(const float2 *state, int n, int cb, double *out, cudaStream_t stream);
+cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni, int shots, int64_t *out,
+                          void *scratch, cudaStream_t stream);
+size_t reduce_scratch_bytes(int n, int chunk_bits);
+cudaError_t take_device_status(int *out);
+}  // namespace qsv
+
+static thread_local std::string t_err;
+static thread_local long long t_launches = 0;
+static std::mutex g_launch_mu;         // serialises first-use kernel attribute setup
+static int g_lo_merge = 4;             // merged sweeps keep sub-blocks of >= 2^4 amplitudes (128 B)
+
+static const int QSV_CHUNK_BITS = 12;  // sampler chunk: 2^12 amplitudes (host/sv/runtime.py:47 chunk_bits=12)
+static int chunk_bits_for(int n) { return n < QSV_CHUNK_BITS ? n : QSV_CHUNK_BITS; }
+static const int QSV_N_MIN = 10;
+static const int QSV_N_MAX = 34;
+
+static int fail(int code, const std::string &msg) {
+    t_err = msg;
+    return code;
+}
+static int cuda_fail(cudaError_t e, const char *what) {
+    return fail(QSV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
+}
+
+extern "C" {
+
+int qsv_version(void) { return 100; }
+
+const char *qsv_last_error(void) { return t_err.c_str(); }
+
+int qsv_set_lo_merge(int lo) {
+    if (lo < QSV_LO_MIN || lo > 13) return fail(QSV_ERR_INVALID_ARG, "lo_merge out of [3, 13]");
+    g_lo_merge = lo;
+    return QSV_OK;
+}
+
+int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap) {
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    std::vector<qsv::PhysPass> passes;
+    std::string err;
+    int rc = qsv::decode_segment(seg, nwords, n, passes, err);
+    if (rc) return fail(rc, err);
+    std::vector<QsvSweep> sweeps;
+    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    if (rc) return fail(rc, err);
+    return qsv::serialize(sweeps, out, cap);
+}
+
+int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int dtype, void *stream) {
+    if (!state) return fail(QSV_ERR_INVALID_ARG, "state is null");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 segments are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    std::vector<qsv::PhysPass> passes;
+    std::string err;
+    int rc = qsv::decode_segment(seg, nwords, n, passes, err);
+    if (rc) return fail(rc, err);
+    std::vector<QsvSweep> sweeps;
+    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    if (rc) return fail(rc, err);
+    const int nsm = sm_count();
+    std::lock_guard<std::mutex> lk(g_launch_mu);
+    for (const QsvSweep &sw : sweeps) {
+        cudaError_t e = qsv::launch_sweep((float2 *)state, sw, nsm, (cudaStream_t)stream);
+        if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+        t_launches++;
+    }
+    return QSV_OK;
+}
+
+int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, void *stream) {
+    if (!src || !dst || !perm) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    if (src == dst) return fail(QSV_ERR_INVALID_ARG, "remap is out of place: src == dst");
+    bool seen[64] = {false};
+    for (int j = 0; j < n; j++) {
+        if (perm[j] < 0 || perm[j] >= n || seen[perm[j]]) return fail(QSV_ERR_INVALID_ARG, "perm is not a permutation");
+        seen[perm[j]] = true;
+    }
+    cudaError_t e = qsv::launch_remap((const float2 *)src, (float2 *)dst, n, perm, sm_count(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "remap launch");
+    t_launches++;
+    return QSV_OK;
+}
+
+int qsv_zero_state(void *state, int n, int dtype, void *stream) {
+    if (!state) return fail(QSV_ERR_INVALID_ARG, "state is null");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < 1 || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of range");
+    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)8 << n, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "memset");
+    e = qsv::launch_set_amp0((float2 *)state, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "init launch");
+    t_launches++;
+    return QSV_OK;
+}
+
+size_t qsv_reduce_scratch_bytes(int n) {
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return 0;
+    return qsv::reduce_scratch_bytes(n, chunk_bits_for(n));
+}
+
+int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *scratch, size_t scratch_bytes,
+                   void *stream) {
+    if (!state || !out_dev || !scratch) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    if (scratch_bytes < qsv_reduce_scratch_bytes(n)) return fail(QSV_ERR_SCRATCH, "scratch too small");
+    cudaError_t e = qsv::launch_reduce((const float2 *)state, n, out_dev, scratch, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "reduce launch");
+    t_launches += 2;
+    return QSV_OK;
+}
+
+int qsv_chunk_probs_f64(const void *state, int n, int dtype, int chunk_bits, double *out_dev, void *stream) {
+    if (!state || !out_dev) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX || chunk_bits < 0 || chunk_bits > n)
+        return fail(QSV_ERR_INVALID_ARG, "n or chunk_bits out of range");
+    cudaError_t e = qsv::launch_chunk_probs((const float2 *)state, n, chunk_bits, out_dev, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "chunk launch");
+    t_launches++;
+    return QSV_OK;
+}
+
+int qsv_sample_f64(const void *state, int n, int dtype, const double *uniforms_dev, int shots, int64_t *out_dev,
+                   void *scratch, size_t scratch_bytes, void *stream) {
+    if (!state || !scratch || (shots > 0 && (!uniforms_dev || !out_dev))) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX || shots < 0) return fail(QSV_ERR_INVALID_ARG, "n or shots out of range");
+    if (scratch_bytes < qsv_reduce_scratch_bytes(n)) return fail(QSV_ERR_SCRATCH, "scratch too small");
+    cudaError_t e = qsv::launch_sample((const float2 *)state, n, chunk_bits_for(n), uniforms_dev, shots, out_dev, scratch,
+                                       (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sample launch");
+    t_launches += 3;
+    return QSV_OK;
+}
+
+int qsv_device_status(int *status) {
+    if (!status) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    int v = 0;
+    cudaError_t e = qsv::take_device_status(&v);
+    if (e != cudaSuccess) return cuda_fail(e, "device status");
+    *status = v;
+    return QSV_OK;
+}
+
+long long qsv_take_launch_count(void) {
+    long long v = t_launches;
+    t_launches = 0;
+    return v;
+}
+
+}  // extern "C"

@@ -1,0 +1,72 @@
+// qsv_plan.h -- the sweep plan: how the engine executes a QSV2 segment (shared by host and device).
+//
+// A QSV2 pass (host/sv/isa.py:13-21) applies its MUX2 ops to every 2^k-amplitude tile of one qubit
+// window. Consecutive passes whose combined qubit set fits one engine window are executed as ONE sweep
+// over HBM: applying pass A's ops and then pass B's ops tile by tile gives exactly the amplitudes that
+// pass-by-pass execution gives, because every op only reads and writes amplitude pairs inside the tile
+// and ops are applied in program order.
+//
+// Sweep window: W = {0, ..., lo-1} U H (H sorted, all >= lo), |W| = KW. Tile bit i <-> physical qubit
+// W[i]. A tile is 2^(KW - lo) sub-blocks of 2^lo contiguous amplitudes (sub-block s at
+// base | pdep(s, H)); tile T's base is pdep(T, free bits), the free bits being the qubits outside W.
+//
+// In-tile execution: consumer thread layout per phase (KW = 1 + 3 + 2 + RB + WB tile bits):
+//   tile bit 0          -> the two amplitudes of one float4 (component pair)
+//   tile bits 1, 2, 3   -> lane bits 0, 1, 2 (conflict-free 128-bit shared-memory accesses)
+//   lane_bits[0..1]     -> lane bits 3, 4
+//   reg_bits[0..RB-1]   -> register index bits (2^RB float4 per thread)
+//   warp_bits[..]       -> warp index bits
+// An op can run in a phase when its target is tile bit 0..3, a register bit or a lane bit of that phase;
+// controls may sit anywhere in the window.
+#pragma once
+#include <stdint.h>
+
+#define QSV_KW_MAX 13
+#define QSV_RB_MAX 4
+#define QSV_WB_MAX 3
+#define QSV_MAX_SWEEP_OPS 96
+#define QSV_MAX_PHASES 24
+#define QSV_LO_MIN 3            // smallest sub-block: 2^3 amplitudes = 64 bytes (QSV2 guarantees k-m >= 3)
+
+// matrix classes (host-detected, exact comparisons): the specialised forms give the same values as
+// the dense fused-multiply-add chain
+#define QSV_M_DENSE 0
+#define QSV_M_DIAG 1            // off-diagonal entries are (+/-)0
+#define QSV_M_IDENT 2           // identity: pair left unchanged
+#define QSV_M_XSWAP 3           // [[0,1],[1,0]]: the two amplitudes are exchanged
+
+// where the target of an op lives in its phase
+#define QSV_SLOT_COMP 0         // tile bit 0 (inside a float4)
+#define QSV_SLOT_REG0 1         // 1 + r: register bit r
+#define QSV_SLOT_LANE0 8        // 8 + l: lane bit l (warp shuffle)
+
+struct QsvOp {
+    float m0[8];                // M0 = m00 m01 m10 m11 as (re, im)
+    float m1[8];                // M1
+    uint32_t cmask;             // control mask over tile bits (0 = no controls)
+    uint8_t cls0, cls1;         // QSV_M_* of M0, M1
+    uint8_t slot;               // QSV_SLOT_*
+    uint8_t tbit;               // target tile bit
+};
+
+struct QsvPhase {
+    uint8_t reg_bits[QSV_RB_MAX];
+    uint8_t lane_bits[2];
+    uint8_t warp_bits[QSV_WB_MAX];
+    uint8_t op_begin, op_end;
+    uint8_t pad[4];
+};
+
+struct QsvSweep {
+    int32_t n;                  // state qubits
+    int32_t kw;                 // window size (tile = 2^kw amplitudes)
+    int32_t lo;                 // contiguous low bits of the window
+    int32_t nh;                 // |H|
+    uint8_t H[QSV_KW_MAX];      // high window qubits, ascending
+    uint8_t pad[3];
+    int64_t ntiles;             // 2^(n - kw)
+    int32_t nphases;
+    int32_t nops;
+    QsvPhase phases[QSV_MAX_PHASES];
+    QsvOp ops[QSV_MAX_SWEEP_OPS];
+};

@@ -1,0 +1,264 @@
+// qsv_planner.cpp -- host decode of QSV2 segments and construction of the sweep plan.
+//
+// decode_segment follows the stream layout of host/sv/isa.py:1-32 and the reader in host/sv/model.py:7-22
+// (validation mirrors what the reference engine assumes: magic, L, k <= L, m <= MAX_HIGH, <= 64 ops per
+// pass, opcode MUX2, record bounds). Each op is converted from pass-tile coordinates to physical qubits
+// (tile qubit q < k-m is physical q, tile qubit k-m+i is h_i; host/sv/isa.py:14-15).
+#include "qsv_planner.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace qsv {
+
+static inline float f_of(int32_t w) {
+    float f;
+    std::memcpy(&f, &w, 4);
+    return f;
+}
+
+int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPass> &out, std::string &err) {
+    out.clear();
+    if (!seg || nwords < QSV2_HDR_WORDS) { err = "segment shorter than its header"; return QSV_ERR_BAD_STREAM; }
+    if ((uint32_t)seg[0] != QSV2_MAGIC) { err = "bad QSV2 magic"; return QSV_ERR_BAD_STREAM; }
+    const int L = seg[1], npass = seg[2], k = seg[3];
+    if (L != n) { err = "segment L (" + std::to_string(L) + ") != state qubits (" + std::to_string(n) + ")"; return QSV_ERR_BAD_STREAM; }
+    if (k < 1 || k > L || npass < 0) { err = "bad segment header (k, n_passes)"; return QSV_ERR_BAD_STREAM; }
+    size_t pos = QSV2_HDR_WORDS;
+    for (int p = 0; p < npass; p++) {
+        if (pos + QSV2_PASS_WORDS > nwords) { err = "truncated pass header"; return QSV_ERR_BAD_STREAM; }
+        const int m = seg[pos], nops = seg[pos + 3];
+        const int h[4] = {seg[pos + 1], seg[pos + 2], seg[pos + 4], seg[pos + 5]};
+        if (m < 0 || m > 4 || m > k || nops < 0 || nops > QSV2_MAX_OPS) { err = "bad pass header"; return QSV_ERR_BAD_STREAM; }
+        for (int i = 0; i < m; i++) {
+            if (h[i] < k - m || h[i] >= L) { err = "high qubit outside [k-m, L)"; return QSV_ERR_BAD_STREAM; }
+            for (int j = 0; j < i; j++)
+                if (h[j] == h[i]) { err = "repeated high qubit"; return QSV_ERR_BAD_STREAM; }
+        }
+        pos += QSV2_PASS_WORDS;
+        PhysPass pp;
+        for (int o = 0; o < nops; o++) {
+            if (pos + QSV2_OP_WORDS > nwords) { err = "truncated op record"; return QSV_ERR_BAD_STREAM; }
+            const int32_t *rec = seg + pos;
+            if (rec[0] != QSV2_OP_MUX2) { err = "unknown opcode " + std::to_string(rec[0]); return QSV_ERR_BAD_STREAM; }
+            const int t = rec[1];
+            const uint32_t cm = (uint32_t)rec[2];
+            if (t < 0 || t >= k || (k < 32 && (cm >> k))) { err = "op target/cmask outside the tile"; return QSV_ERR_BAD_STREAM; }
+            auto phys = [&](int tq) { return tq < k - m ? tq : h[tq - (k - m)]; };
+            PhysOp op;
+            op.t = phys(t);
+            op.cmask = 0;
+            for (int b = 0; b < k; b++)
+                if ((cm >> b) & 1) op.cmask |= 1ull << phys(b);
+            // a control on the target bit can never be set in i0, so M1 is never selected: keep that
+            // meaning by recording it (the engine tests i0, which has the target bit clear)
+            for (int e = 0; e < 8; e++) { op.m0[e] = f_of(rec[8 + e]); op.m1[e] = f_of(rec[16 + e]); }
+            pp.ops.push_back(op);
+            pos += QSV2_OP_WORDS;
+        }
+        out.push_back(std::move(pp));
+    }
+    if (pos != nwords) { err = "trailing words after the last pass"; return QSV_ERR_BAD_STREAM; }
+    return QSV_OK;
+}
+
+int layout_for_kw(int kw, int *rb, int *wb) {
+    switch (kw) {
+        case 13: *rb = 4; *wb = 3; return 0;
+        case 12: *rb = 4; *wb = 2; return 0;
+        case 11: *rb = 3; *wb = 2; return 0;
+        case 10: *rb = 2; *wb = 2; return 0;
+        default: return -1;
+    }
+}
+
+static uint64_t op_qubits(const PhysOp &op) { return op.cmask | (1ull << op.t); }
+
+static int window_lo(uint64_t qset, int n, int kw) {
+    // largest lo with lo + |{q in qset : q >= lo}| <= kw
+    int best = -1;
+    for (int lo = 0; lo <= std::min(n, kw); lo++) {
+        int cnt = __builtin_popcountll(lo >= 64 ? 0 : (qset >> lo));
+        if (lo + cnt <= kw) best = lo;
+    }
+    return best;
+}
+
+static uint8_t classify(const float *m) {
+    auto z = [](float x) { return x == 0.0f; };
+    const bool offz = z(m[2]) && z(m[3]) && z(m[4]) && z(m[5]);
+    if (offz && m[0] == 1.0f && z(m[1]) && m[6] == 1.0f && z(m[7])) return QSV_M_IDENT;
+    if (offz) return QSV_M_DIAG;
+    if (z(m[0]) && z(m[1]) && m[2] == 1.0f && z(m[3]) && m[4] == 1.0f && z(m[5]) && z(m[6]) && z(m[7]))
+        return QSV_M_XSWAP;
+    return QSV_M_DENSE;
+}
+
+static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
+                      QsvSweep &sw, std::string &err) {
+    int rb, wb;
+    if (layout_for_kw(kw, &rb, &wb)) { err = "unsupported window size"; return QSV_ERR_UNSUPPORTED; }
+    std::memset(&sw, 0, sizeof(sw));
+    const int lo = window_lo(qset, n, kw);
+    if (lo < QSV_LO_MIN) { err = "op qubits do not fit one 13-qubit window"; return QSV_ERR_UNSUPPORTED; }
+    sw.n = n;
+    sw.kw = kw;
+    sw.lo = lo;
+    int tile_of[64];
+    for (int q = 0; q < 64; q++) tile_of[q] = -1;
+    for (int q = 0; q < lo; q++) tile_of[q] = q;
+    int nh = 0;
+    for (int q = lo; q < n; q++)
+        if ((qset >> q) & 1) { sw.H[nh] = (uint8_t)q; tile_of[q] = lo + nh; nh++; }
+    sw.nh = nh;
+    sw.ntiles = 1ll << (n - kw);
+    sw.nops = (int)(e - b);
+    // ops in tile coordinates
+    for (size_t i = b; i < e; i++) {
+        QsvOp &o = sw.ops[i - b];
+        const PhysOp &p = ops[i];
+        std::memcpy(o.m0, p.m0, sizeof(o.m0));
+        std::memcpy(o.m1, p.m1, sizeof(o.m1));
+        o.tbit = (uint8_t)tile_of[p.t];
+        o.cmask = 0;
+        for (int q = 0; q < n; q++)
+            if ((p.cmask >> q) & 1) o.cmask |= 1u << tile_of[q];
+        o.cls0 = classify(o.m0);
+        o.cls1 = classify(o.m1);
+        // identical matrices: the selection cannot change any value, so the op runs unconditioned
+        if (std::memcmp(o.m0, o.m1, sizeof(o.m0)) == 0) o.cmask = 0;
+    }
+    // phases: greedy in op order; tile bits >= 4 that are targets need a register or lane slot
+    const int cap = rb + 2;
+    int nph = 0;
+    size_t i = 0;
+    while (i < (size_t)sw.nops) {
+        if (nph >= QSV_MAX_PHASES) { err = "too many phases"; return QSV_ERR_UNSUPPORTED; }
+        size_t j = i;
+        int used[QSV_KW_MAX], cnt[QSV_KW_MAX], nu = 0;
+        while (j < (size_t)sw.nops) {
+            const int tb = sw.ops[j].tbit;
+            if (tb >= 4) {
+                int f = -1;
+                for (int u = 0; u < nu; u++)
+                    if (used[u] == tb) f = u;
+                if (f < 0) {
+                    if (nu == cap) break;
+                    used[nu] = tb; cnt[nu] = 0; f = nu++;
+                }
+                cnt[f]++;
+            }
+            j++;
+        }
+        // order targets by use count (stable): most used go to register bits
+        int order[QSV_KW_MAX];
+        for (int u = 0; u < nu; u++) order[u] = u;
+        std::stable_sort(order, order + nu, [&](int a, int c) { return cnt[a] > cnt[c]; });
+        QsvPhase &ph = sw.phases[nph];
+        bool taken[QSV_KW_MAX] = {false};
+        int slots[QSV_KW_MAX], ns = 0;   // reg bits then lane bits 3, 4 then warp bits
+        for (int u = 0; u < nu; u++) { slots[ns++] = used[order[u]]; taken[used[order[u]]] = true; }
+        // targets beyond rb go to lane slots; unused reg/lane slots and warp slots get the remaining bits
+        int regs[QSV_RB_MAX], nr = 0, lanes[2], nl = 0;
+        for (int u = 0; u < ns; u++) {
+            if (nr < rb) regs[nr++] = slots[u];
+            else lanes[nl++] = slots[u];
+        }
+        int rest[QSV_KW_MAX], nrest = 0;
+        for (int t = 4; t < kw; t++)
+            if (!taken[t]) rest[nrest++] = t;
+        int ri = 0;
+        while (nr < rb) regs[nr++] = rest[ri++];
+        while (nl < 2) lanes[nl++] = rest[ri++];
+        for (int w = 0; w < wb; w++) ph.warp_bits[w] = (uint8_t)rest[ri++];
+        for (int r = 0; r < rb; r++) ph.reg_bits[r] = (uint8_t)regs[r];
+        ph.lane_bits[0] = (uint8_t)lanes[0];
+        ph.lane_bits[1] = (uint8_t)lanes[1];
+        ph.op_begin = (uint8_t)i;
+        ph.op_end = (uint8_t)j;
+        for (size_t o = i; o < j; o++) {
+            QsvOp &op = sw.ops[o];
+            const int tb = op.tbit;
+            if (tb == 0) op.slot = QSV_SLOT_COMP;
+            else if (tb < 4) op.slot = (uint8_t)(QSV_SLOT_LANE0 + tb - 1);
+            else {
+                op.slot = 0xff;
+                for (int r = 0; r < rb; r++)
+                    if (ph.reg_bits[r] == tb) op.slot = (uint8_t)(QSV_SLOT_REG0 + r);
+                for (int l = 0; l < 2; l++)
+                    if (ph.lane_bits[l] == tb) op.slot = (uint8_t)(QSV_SLOT_LANE0 + 3 + l);
+                if (op.slot == 0xff) { err = "internal: target not placed"; return QSV_ERR_UNSUPPORTED; }
+            }
+        }
+        nph++;
+        i = j;
+    }
+    sw.nphases = nph;
+    return QSV_OK;
+}
+
+int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,
+                 std::string &err) {
+    out.clear();
+    std::vector<PhysOp> ops;
+    uint64_t cur = 0;
+    size_t begin = 0;
+    auto flush = [&]() -> int {
+        if (ops.size() > begin) {
+            out.emplace_back();
+            int rc = fill_sweep(ops, begin, ops.size(), cur, n, kw, out.back(), err);
+            if (rc) return rc;
+        }
+        begin = ops.size();
+        cur = 0;
+        return QSV_OK;
+    };
+    for (const PhysPass &p : passes) {
+        if (p.ops.empty()) continue;
+        uint64_t q = 0;
+        for (const PhysOp &o : p.ops) q |= op_qubits(o);
+        const uint64_t merged = cur | q;
+        const size_t nmerged = ops.size() - begin + p.ops.size();
+        const bool fits = window_lo(merged, n, kw) >= lo_merge && nmerged <= QSV_MAX_SWEEP_OPS;
+        if (ops.size() > begin && !fits) {
+            int rc = flush();
+            if (rc) return rc;
+        }
+        ops.insert(ops.end(), p.ops.begin(), p.ops.end());   // a QSV2 pass has <= 64 ops < the sweep budget
+        cur |= q;
+    }
+    return flush();
+}
+
+int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
+    std::vector<int32_t> w;
+    w.push_back((int32_t)sw.size());
+    for (const QsvSweep &s : sw) {
+        int rb = 0, wb = 0;
+        layout_for_kw(s.kw, &rb, &wb);
+        w.push_back(s.kw); w.push_back(s.lo); w.push_back(s.nh);
+        for (int i = 0; i < QSV_KW_MAX; i++) w.push_back(i < s.nh ? s.H[i] : -1);
+        w.push_back(s.nphases); w.push_back(s.nops);
+        for (int p = 0; p < s.nphases; p++) {
+            const QsvPhase &ph = s.phases[p];
+            for (int r = 0; r < QSV_RB_MAX; r++) w.push_back(r < rb ? ph.reg_bits[r] : -1);
+            w.push_back(ph.lane_bits[0]); w.push_back(ph.lane_bits[1]);
+            for (int r = 0; r < QSV_WB_MAX; r++) w.push_back(r < wb ? ph.warp_bits[r] : -1);
+            w.push_back(ph.op_begin); w.push_back(ph.op_end);
+        }
+        for (int o = 0; o < s.nops; o++) {
+            const QsvOp &op = s.ops[o];
+            w.push_back(op.tbit); w.push_back(op.slot); w.push_back((int32_t)op.cmask);
+            w.push_back(op.cls0); w.push_back(op.cls1);
+            int32_t b[8];
+            std::memcpy(b, op.m0, 32);
+            for (int e = 0; e < 8; e++) w.push_back(b[e]);
+            std::memcpy(b, op.m1, 32);
+            for (int e = 0; e < 8; e++) w.push_back(b[e]);
+        }
+    }
+    if (out) std::memcpy(out, w.data(), sizeof(int32_t) * std::min(cap, w.size()));
+    return (int)w.size();
+}
+
+}  // namespace qsv

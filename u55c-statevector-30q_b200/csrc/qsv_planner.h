@@ -1,0 +1,40 @@
+// qsv_planner.h -- host-side decode of QSV2 segments into sweep plans (see qsv_plan.h).
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/qsv_b200.h"
+#include "qsv_plan.h"
+
+#define QSV2_MAGIC 0x51535632u
+#define QSV2_HDR_WORDS 8
+#define QSV2_PASS_WORDS 8
+#define QSV2_OP_WORDS 24
+#define QSV2_OP_MUX2 1
+#define QSV2_MAX_OPS 64
+
+namespace qsv {
+
+// one MUX2 op in physical coordinates
+struct PhysOp {
+    int t;                 // target qubit
+    uint64_t cmask;        // control qubits
+    float m0[8], m1[8];
+};
+struct PhysPass {
+    std::vector<PhysOp> ops;
+};
+
+// Validate a segment for an n-qubit state and convert its ops to physical qubits.
+int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPass> &out, std::string &err);
+// Register/warp bit split of the consumer layout for a window of kw qubits (kw in 10..13).
+int layout_for_kw(int kw, int *rb, int *wb);
+// Merge consecutive passes into sweeps of window kw; merged windows keep >= 2^lo_merge contiguous amps.
+int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,
+                 std::string &err);
+// Flatten a plan into int32 words (layout documented in qsv_b200.h / the planner tests).
+int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap);
+
+}  // namespace qsv

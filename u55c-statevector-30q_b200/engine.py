@@ -1,0 +1,228 @@
+"""ctypes binding of libqsv_b200.so (the C ABI in include/qsv_b200.h) plus device-state helpers.
+
+PyTorch only holds device memory and streams here: states are complex64 CUDA tensors whose storage is
+handed to the C ABI as raw pointers, on the current PyTorch stream. There is no CPU execution path: if
+the library cannot be loaded, or no CUDA device is present, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqsv_b200.so")
+
+QSV_OK = 0
+QSV_C64 = 0
+CHUNK_BITS = 12
+N_MIN, N_MAX = 10, 34
+
+_ERRORS = {-1: "invalid argument", -2: "bad QSV2 stream", -3: "unsupported", -4: "CUDA error", -5: "device fault",
+           -6: "scratch too small"}
+
+
+class QSVError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERRORS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+class BadStream(QSVError, ValueError):
+    pass
+
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load the engine library (built by build.py). Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libqsv_b200.so not found at {path}; build it with build.py (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
+    P, I32, SZ, I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_size_t, ctypes.c_int64
+    sig = {
+        "qsv_version": ([], I32),
+        "qsv_last_error": ([], ctypes.c_char_p),
+        "qsv_run_segment": ([P, ctypes.c_int, P, SZ, ctypes.c_int, P], I32),
+        "qsv_remap": ([P, P, ctypes.c_int, P, ctypes.c_int, P], I32),
+        "qsv_zero_state": ([P, ctypes.c_int, ctypes.c_int, P], I32),
+        "qsv_reduce_scratch_bytes": ([ctypes.c_int], SZ),
+        "qsv_reduce_f64": ([P, ctypes.c_int, ctypes.c_int, P, P, SZ, P], I32),
+        "qsv_chunk_probs_f64": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P], I32),
+        "qsv_sample_f64": ([P, ctypes.c_int, ctypes.c_int, P, ctypes.c_int, P, P, SZ, P], I32),
+        "qsv_plan_segment": ([P, SZ, ctypes.c_int, P, SZ], I32),
+        "qsv_device_status": ([P], I32),
+        "qsv_take_launch_count": ([], ctypes.c_longlong),
+        "qsv_set_lo_merge": ([ctypes.c_int], I32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names of the C ABI functions declared in include/qsv_b200.h."""
+    return ["qsv_version", "qsv_last_error", "qsv_run_segment", "qsv_remap", "qsv_zero_state",
+            "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_chunk_probs_f64", "qsv_sample_f64",
+            "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge"]
+
+
+def _check(rc):
+    if rc != QSV_OK:
+        msg = load().qsv_last_error().decode()
+        if rc == -2:
+            raise BadStream(rc, msg)
+        raise QSVError(rc, msg)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("qsv_b200 needs a CUDA device (B200); none is available")
+    return torch
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _qubits(state):
+    n = state.numel().bit_length() - 1
+    if state.numel() != 1 << n:
+        raise ValueError("state length is not a power of two")
+    return n
+
+
+def new_state(n, device=None, zero=True, stream=None):
+    """Allocate a complex64 device state of 2^n amplitudes (|0...0> unless zero=False)."""
+    torch = _torch()
+    t = torch.empty(1 << n, dtype=torch.complex64, device=device or "cuda")
+    if zero:
+        zero_state(t, stream)
+    return t
+
+
+def zero_state(state, stream=None):
+    _check(load().qsv_zero_state(_ptr(state), _qubits(state), QSV_C64, _stream(stream)))
+
+
+def run_segment(state, seg, stream=None):
+    """Execute one QSV2 segment (np.int32 words) in place on a complex64 CUDA tensor."""
+    assert state.is_cuda and state.dtype.is_complex and state.element_size() == 8 and state.is_contiguous()
+    w = np.ascontiguousarray(seg, dtype=np.int32)
+    _check(load().qsv_run_segment(_ptr(state), _qubits(state), w.ctypes.data_as(ctypes.c_void_p), w.size,
+                                  QSV_C64, _stream(stream)))
+
+
+def remap(src, dst, perm, stream=None):
+    """dst <- src with index bits permuted, perm[new] = old. src and dst are distinct tensors."""
+    p = np.ascontiguousarray(perm, dtype=np.int32)
+    n = _qubits(src)
+    if len(p) != n or dst.numel() != src.numel():
+        raise ValueError("permutation length / state size mismatch")
+    _check(load().qsv_remap(_ptr(src), _ptr(dst), n, p.ctypes.data_as(ctypes.c_void_p), QSV_C64, _stream(stream)))
+
+
+def scratch_bytes(n):
+    return int(load().qsv_reduce_scratch_bytes(n))
+
+
+def new_scratch(n, device=None):
+    torch = _torch()
+    return torch.empty(scratch_bytes(n), dtype=torch.uint8, device=device or "cuda")
+
+
+def reduce_f64(state, out=None, scratch=None, stream=None):
+    """Device FP64 reductions: tensor [sum |a|^2, <Z_0>, ..., <Z_{n-1}>] (float64, on the device)."""
+    torch = _torch()
+    n = _qubits(state)
+    out = torch.empty(n + 1, dtype=torch.float64, device=state.device) if out is None else out
+    scratch = new_scratch(n, state.device) if scratch is None else scratch
+    _check(load().qsv_reduce_f64(_ptr(state), n, QSV_C64, _ptr(out), _ptr(scratch), scratch.numel(), _stream(stream)))
+    return out
+
+
+def chunk_probs_f64(state, chunk_bits=CHUNK_BITS, stream=None):
+    torch = _torch()
+    n = _qubits(state)
+    out = torch.empty(1 << (n - chunk_bits), dtype=torch.float64, device=state.device)
+    _check(load().qsv_chunk_probs_f64(_ptr(state), n, QSV_C64, chunk_bits, _ptr(out), _stream(stream)))
+    return out
+
+
+def sample_f64(state, uniforms, scratch=None, stream=None):
+    """Physical indices (int64 device tensor) of Born-rule samples, one per uniform in [0, 1)."""
+    torch = _torch()
+    n = _qubits(state)
+    u = uniforms if isinstance(uniforms, torch.Tensor) else torch.as_tensor(np.asarray(uniforms, dtype=np.float64))
+    u = u.to(device=state.device, dtype=torch.float64).contiguous()
+    out = torch.empty(u.numel(), dtype=torch.int64, device=state.device)
+    scratch = new_scratch(n, state.device) if scratch is None else scratch
+    _check(load().qsv_sample_f64(_ptr(state), n, QSV_C64, _ptr(u), u.numel(), _ptr(out), _ptr(scratch),
+                                 scratch.numel(), _stream(stream)))
+    return out
+
+
+def plan_segment(seg, n):
+    """Decode a segment into the engine's sweep plan (host only): list of dicts."""
+    L = load()
+    w = np.ascontiguousarray(seg, dtype=np.int32)
+    need = L.qsv_plan_segment(w.ctypes.data_as(ctypes.c_void_p), w.size, n, None, 0)
+    if need < 0:
+        _check(need)
+    buf = np.zeros(need, dtype=np.int32)
+    L.qsv_plan_segment(w.ctypes.data_as(ctypes.c_void_p), w.size, n, buf.ctypes.data_as(ctypes.c_void_p), need)
+    return _parse_plan(buf, n)
+
+
+def _parse_plan(w, n):
+    rb_of = {13: 4, 12: 4, 11: 3, 10: 2}
+    pos = 1
+    sweeps = []
+    for _ in range(int(w[0])):
+        kw, lo, nh = (int(x) for x in w[pos:pos + 3])
+        pos += 3
+        H = [int(x) for x in w[pos:pos + 13] if x >= 0]
+        pos += 13
+        nph, nops = int(w[pos]), int(w[pos + 1])
+        pos += 2
+        phases = []
+        for _ in range(nph):
+            rec = [int(x) for x in w[pos:pos + 11]]
+            pos += 11
+            phases.append(dict(reg_bits=[r for r in rec[:4] if r >= 0][:rb_of[kw]], lane_bits=rec[4:6],
+                               warp_bits=[r for r in rec[6:9] if r >= 0], op_begin=rec[9], op_end=rec[10]))
+        ops = []
+        for _ in range(nops):
+            tbit, slot, cmask, c0, c1 = (int(x) for x in w[pos:pos + 5])
+            m = w[pos + 5:pos + 21].view(np.float32).copy()
+            pos += 21
+            ops.append(dict(tbit=tbit, slot=slot, cmask=cmask & 0xFFFFFFFF, cls0=c0, cls1=c1, m0=m[:8], m1=m[8:]))
+        sweeps.append(dict(kw=kw, lo=lo, H=H, window=list(range(lo)) + H, phases=phases, ops=ops))
+    return sweeps
+
+
+def device_status():
+    v = ctypes.c_int(0)
+    _check(load().qsv_device_status(ctypes.byref(v)))
+    return v.value
+
+
+def take_launch_count():
+    return int(load().qsv_take_launch_count())
+
+
+def set_lo_merge(lo):
+    _check(load().qsv_set_lo_merge(int(lo)))
