@@ -51,11 +51,16 @@ def _gpu_segment(torch, x, seg):
 def test_golden_fixture_segments(torch):
     js = json.load(open(os.path.join(GOLD, "streams.json")))
     st = np.load(os.path.join(GOLD, "model_states.npz"))
+    checked = 0
     for c in js["segments"]:
+        if c["n"] < engine.N_MIN:
+            continue            # the engine's smallest state is 2^10 (the runtime pads smaller circuits)
         x, w = st[c["key"] + "_in"], st[c["key"] + "_words"]
         y = _gpu_segment(torch, x, w)
+        checked += 1
         assert np.array_equal(y, orc.run_segment(x.copy(), w)), c
         assert np.max(np.abs(y - st[c["key"] + "_out"])) <= 2e-6, c
+    assert checked >= 4
 
 
 CASES = [
