@@ -105,6 +105,14 @@ QSV_API long long qsv_take_launch_count(void);
  * contiguous (lo in [3, 13]; default 4 = 128 bytes). Larger values merge fewer passes. Process-wide. */
 QSV_API int qsv_set_lo_merge(int lo);
 
+/* Tuning knob (no reference counterpart): consumer layout of the 13-qubit sweep kernel, 4 register bits
+ * per thread with 8 consumer warps (default) or 3 with 16. Values are identical either way. */
+QSV_API int qsv_set_layout13(int rb);
+
+/* Tuning knob (no reference counterpart): how many op targets a phase may place on lane bits (warp
+ * shuffles) instead of starting a new phase, 0..2 (default 2). Values are identical either way. */
+QSV_API int qsv_set_phase_lanes(int k);
+
 #ifdef __cplusplus
 }
 #endif

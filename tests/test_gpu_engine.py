@@ -223,3 +223,22 @@ def test_bad_stream_leaves_state(torch):
         engine.run_segment(t, bad)
     h = t.cpu().numpy()
     assert h[0] == 1 and np.count_nonzero(h) == 1
+
+
+@pytest.mark.parametrize("rb", [3, 4])
+def test_layout13_variants_exact(torch, rb):
+    """Both consumer layouts of the 13-qubit kernel give the oracle's values."""
+    try:
+        engine.set_layout13(rb)
+        for n, qc in ((18, gen.random_layer(18, 6, 31)), (16, gen.zoo(16, 7)), (17, gen.random_layer_ccx(17, 4, 9))):
+            prog, fmap, st = q.compile_circuit(qc, n, 12)
+            x = _rand_state(n, 11)
+            for kind, seg in prog:
+                if kind == "segment":
+                    y = _gpu_segment(torch, x, seg)
+                    assert np.array_equal(y, orc.run_segment(x.copy(), seg)), (rb, n)
+                    x = y
+                else:
+                    x = orc.remap(x, seg)
+    finally:
+        engine.set_layout13(4)

@@ -62,6 +62,16 @@ int qsv_set_lo_merge(int lo) {
     return QSV_OK;
 }
 
+int qsv_set_layout13(int rb) {
+    if (qsv::set_rb13(rb)) return fail(QSV_ERR_INVALID_ARG, "13-qubit layout takes 3 or 4 register bits");
+    return QSV_OK;
+}
+
+int qsv_set_phase_lanes(int k) {
+    if (qsv::set_phase_lanes(k)) return fail(QSV_ERR_INVALID_ARG, "phase lane targets must be 0, 1 or 2");
+    return QSV_OK;
+}
+
 int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap) {
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     std::vector<qsv::PhysPass> passes;

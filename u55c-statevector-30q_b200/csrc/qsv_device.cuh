@@ -107,6 +107,10 @@ __device__ __forceinline__ void pair_apply(float &x0r, float &x0i, float &x1r, f
         diag_own(y0r, y0i, m[0], m[1], x0r, x0i);
         diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
         x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if (cls == QSV_M_DIAG1) {
+        float y1r, y1i;
+        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
+        x1r = y1r; x1i = y1i;
     } else if (cls == QSV_M_XSWAP) {
         float t = x0r; x0r = x1r; x1r = t;
         t = x0i; x0i = x1i; x1i = t;

@@ -10,8 +10,14 @@
 // W[i]. A tile is 2^(KW - lo) sub-blocks of 2^lo contiguous amplitudes (sub-block s at
 // base | pdep(s, H)); tile T's base is pdep(T, free bits), the free bits being the qubits outside W.
 //
+// Tile staging: with long sub-blocks (lo >= QSV_TMA_TENSOR_LO) one bulk-async copy per sub-block; with
+// short ones a single tensor-map TMA box per tile. The tensor map views the state as up to 5 dims, one per
+// run of consecutive window bits (the low run [0, lo) and each run of H); every dim also spans the free
+// bits directly above its run, so a tile's free bits become box coordinates: coordinate of dim d =
+// (next tdim_free[d] bits of T) << tdim_box[d].
+//
 // In-tile execution: consumer thread layout per phase (KW = 1 + 3 + 2 + RB + WB tile bits):
-//   tile bit 0          -> the two amplitudes of one float4 (component pair)
+//   tile bit 0          -> the two halves of one float4 (a thread keeps them packed as re/im float2 pairs)
 //   tile bits 1, 2, 3   -> lane bits 0, 1, 2 (conflict-free 128-bit shared-memory accesses)
 //   lane_bits[0..1]     -> lane bits 3, 4
 //   reg_bits[0..RB-1]   -> register index bits (2^RB float4 per thread)
@@ -23,17 +29,39 @@
 
 #define QSV_KW_MAX 13
 #define QSV_RB_MAX 4
-#define QSV_WB_MAX 3
+#define QSV_WB_MAX 4
 #define QSV_MAX_SWEEP_OPS 96
 #define QSV_MAX_PHASES 24
 #define QSV_LO_MIN 3            // smallest sub-block: 2^3 amplitudes = 64 bytes (QSV2 guarantees k-m >= 3)
+#define QSV_TMA_TENSOR_LO 9     // sub-blocks shorter than 2^9 amplitudes are staged with a tensor-map box
+#define QSV_TMA_MAX_RANK 5
 
-// matrix classes (host-detected, exact comparisons): the specialised forms give the same values as
-// the dense fused-multiply-add chain
+// matrix classes (host-detected, exact comparisons). The specialised forms give the same values as the
+// dense fused-multiply-add chain (the skipped terms are exact zeros).
 #define QSV_M_DENSE 0
 #define QSV_M_DIAG 1            // off-diagonal entries are (+/-)0
 #define QSV_M_IDENT 2           // identity: pair left unchanged
 #define QSV_M_XSWAP 3           // [[0,1],[1,0]]: the two amplitudes are exchanged
+#define QSV_M_DIAG1 4           // diag(1, d): only the bit-1 amplitude changes
+
+// op kinds
+#define QSV_K_UNI 0             // one matrix (M0) for every pair
+#define QSV_K_CTRL 1            // M0 = identity: pairs whose controls are all set get M1
+#define QSV_K_MUX 2             // general: M1 where the controls are set, M0 elsewhere (dense math)
+
+// code path of an op (host-chosen from kind, class and controls): one tight loop per variant
+#define QSV_V_SKIP 0            // identity everywhere
+#define QSV_V_UNI_DENSE 1       // y = M0 x
+#define QSV_V_UNI_DIAG 2        // y0 = m00 x0, y1 = m11 x1
+#define QSV_V_UNI_SWAP 3        // exchange
+#define QSV_V_CTRL_DENSE 4      // y = M1 x where selected (M0 = I)
+#define QSV_V_CTRL_DIAG1 5      // y1 = m11 x1 where selected (M0 = I, M1 = diag(1, d))
+#define QSV_V_CTRL_SWAP 6       // exchange where selected (M0 = I, M1 = X)
+#define QSV_V_MUX 7             // general selection, per-pair coefficient select, dense arithmetic
+// controlled ops whose controls vary across the lanes of a warp: selects instead of branches
+#define QSV_V_CTRL_DENSE_SEL 8
+#define QSV_V_CTRL_DIAG1_SEL 9
+#define QSV_V_CTRL_SWAP_SEL 10
 
 // where the target of an op lives in its phase
 #define QSV_SLOT_COMP 0         // tile bit 0 (inside a float4)
@@ -44,9 +72,16 @@ struct QsvOp {
     float m0[8];                // M0 = m00 m01 m10 m11 as (re, im)
     float m1[8];                // M1
     uint32_t cmask;             // control mask over tile bits (0 = no controls)
+    uint32_t cm_thr;            // the part of cmask on lane / warp tile bits (tested on the thread base)
+    uint8_t cm_reg;             // the part of cmask on register bits, as a mask over the register index
+    uint8_t cm_c;               // 1 if tile bit 0 is a control
+    uint8_t kind;               // QSV_K_*
+    uint8_t cls;                // QSV_M_* of the matrix the kind applies (M0 for UNI, M1 for CTRL)
     uint8_t cls0, cls1;         // QSV_M_* of M0, M1
     uint8_t slot;               // QSV_SLOT_*
     uint8_t tbit;               // target tile bit
+    uint8_t variant;            // QSV_V_*
+    uint8_t pad[3];
 };
 
 struct QsvPhase {
@@ -63,7 +98,10 @@ struct QsvSweep {
     int32_t lo;                 // contiguous low bits of the window
     int32_t nh;                 // |H|
     uint8_t H[QSV_KW_MAX];      // high window qubits, ascending
-    uint8_t pad[3];
+    uint8_t tma_rank;           // 0: bulk copies per sub-block; 2..5: one tensor-map box per tile
+    uint8_t tdim_free[QSV_TMA_MAX_RANK];   // free bits of T folded into each tensor dim (low dim first)
+    uint8_t tdim_box[QSV_TMA_MAX_RANK];    // log2 box extent of each tensor dim
+    uint8_t pad[4];
     int64_t ntiles;             // 2^(n - kw)
     int32_t nphases;
     int32_t nops;

@@ -62,9 +62,24 @@ int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPas
     return QSV_OK;
 }
 
+static int g_rb13 = 4;      // register bits of the 13-qubit layout: 4 (256 consumer threads) or 3 (512)
+static int g_phase_lanes = 2;   // targets (tile bits >= 4) a phase may place on lane bits 3, 4 (0..2)
+
+int set_phase_lanes(int k) {
+    if (k < 0 || k > 2) return -1;
+    g_phase_lanes = k;
+    return 0;
+}
+
+int set_rb13(int rb) {
+    if (rb != 3 && rb != 4) return -1;
+    g_rb13 = rb;
+    return 0;
+}
+
 int layout_for_kw(int kw, int *rb, int *wb) {
     switch (kw) {
-        case 13: *rb = 4; *wb = 3; return 0;
+        case 13: *rb = g_rb13; *wb = 13 - 6 - g_rb13; return 0;
         case 12: *rb = 4; *wb = 2; return 0;
         case 11: *rb = 3; *wb = 2; return 0;
         case 10: *rb = 2; *wb = 2; return 0;
@@ -88,10 +103,34 @@ static uint8_t classify(const float *m) {
     auto z = [](float x) { return x == 0.0f; };
     const bool offz = z(m[2]) && z(m[3]) && z(m[4]) && z(m[5]);
     if (offz && m[0] == 1.0f && z(m[1]) && m[6] == 1.0f && z(m[7])) return QSV_M_IDENT;
+    if (offz && m[0] == 1.0f && z(m[1])) return QSV_M_DIAG1;
     if (offz) return QSV_M_DIAG;
     if (z(m[0]) && z(m[1]) && m[2] == 1.0f && z(m[3]) && m[4] == 1.0f && z(m[5]) && z(m[6]) && z(m[7]))
         return QSV_M_XSWAP;
     return QSV_M_DENSE;
+}
+
+// Tensor-map staging for windows with short contiguous runs: one dim per chunk (<= 8 bits) of each run of
+// window bits, each spanning the free bits up to the next window bit. Returns the rank, 0 if it does not fit.
+static int tma_dims(const QsvSweep &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart) {
+    if (sw.lo >= QSV_TMA_TENSOR_LO) return 0;
+    int wb[QSV_KW_MAX], nw = 0;            // window bits ascending
+    for (int q = 0; q < sw.lo; q++) wb[nw++] = q;
+    for (int i = 0; i < sw.nh; i++) wb[nw++] = sw.H[i];
+    int rank = 0, i = 0;
+    while (i < nw) {
+        int start = wb[i], len = 1;
+        while (i + len < nw && wb[i + len] == start + len && len < 8) len++;
+        const int next = (i + len < nw) ? wb[i + len] : sw.n;
+        const int fr = next - (start + len);
+        if (rank == QSV_TMA_MAX_RANK || len + fr > 31) return 0;
+        tstart[rank] = (uint8_t)start;
+        tbox[rank] = (uint8_t)len;
+        tfree[rank] = (uint8_t)fr;
+        rank++;
+        i += len;
+    }
+    return rank;
 }
 
 static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
@@ -125,11 +164,38 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
             if ((p.cmask >> q) & 1) o.cmask |= 1u << tile_of[q];
         o.cls0 = classify(o.m0);
         o.cls1 = classify(o.m1);
-        // identical matrices: the selection cannot change any value, so the op runs unconditioned
-        if (std::memcmp(o.m0, o.m1, sizeof(o.m0)) == 0) o.cmask = 0;
+        // identical matrices, or a control on the target bit (i0 never has it set): M1 is never
+        // selected / cannot change any value, so the op runs unconditioned with M0
+        if (std::memcmp(o.m0, o.m1, sizeof(o.m0)) == 0 || ((o.cmask >> o.tbit) & 1)) {
+            o.cmask = 0;
+            std::memcpy(o.m1, o.m0, sizeof(o.m0));
+            o.cls1 = o.cls0;
+        }
+        if (o.cmask == 0) { o.kind = QSV_K_UNI; o.cls = o.cls0; }
+        else if (o.cls0 == QSV_M_IDENT) { o.kind = QSV_K_CTRL; o.cls = o.cls1; }
+        else { o.kind = QSV_K_MUX; o.cls = QSV_M_DENSE; }
+        o.cm_c = (uint8_t)(o.cmask & 1u);
+        // code path; the dense arithmetic gives the same values on diagonal / permutation matrices
+        if (o.kind == QSV_K_UNI) {
+            o.variant = o.cls == QSV_M_IDENT ? QSV_V_SKIP
+                        : o.cls == QSV_M_XSWAP ? QSV_V_UNI_SWAP
+                        : (o.cls == QSV_M_DIAG || o.cls == QSV_M_DIAG1) ? QSV_V_UNI_DIAG : QSV_V_UNI_DENSE;
+        } else if (o.kind == QSV_K_CTRL && !o.cm_c) {
+            o.variant = o.cls == QSV_M_IDENT ? QSV_V_SKIP
+                        : o.cls == QSV_M_XSWAP ? QSV_V_CTRL_SWAP
+                        : o.cls == QSV_M_DIAG1 ? QSV_V_CTRL_DIAG1 : QSV_V_CTRL_DENSE;
+        } else {
+            o.variant = QSV_V_MUX;
+        }
+    }
+    {
+        uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
+        const int r = tma_dims(sw, tfree, tbox, tstart);
+        sw.tma_rank = (uint8_t)r;
+        for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
     }
     // phases: greedy in op order; tile bits >= 4 that are targets need a register or lane slot
-    const int cap = rb + 2;
+    const int cap = rb + g_phase_lanes;
     int nph = 0;
     size_t i = 0;
     while (i < (size_t)sw.nops) {
@@ -176,6 +242,8 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         ph.lane_bits[1] = (uint8_t)lanes[1];
         ph.op_begin = (uint8_t)i;
         ph.op_end = (uint8_t)j;
+        uint32_t regmask = 0;
+        for (int r = 0; r < rb; r++) regmask |= 1u << ph.reg_bits[r];
         for (size_t o = i; o < j; o++) {
             QsvOp &op = sw.ops[o];
             const int tb = op.tbit;
@@ -188,6 +256,19 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
                 for (int l = 0; l < 2; l++)
                     if (ph.lane_bits[l] == tb) op.slot = (uint8_t)(QSV_SLOT_LANE0 + 3 + l);
                 if (op.slot == 0xff) { err = "internal: target not placed"; return QSV_ERR_UNSUPPORTED; }
+            }
+            // control split for this phase's layout: register-index part, tile-bit-0 part, thread part
+            op.cm_reg = 0;
+            for (int r = 0; r < rb; r++)
+                if ((op.cmask >> ph.reg_bits[r]) & 1) op.cm_reg |= (uint8_t)(1u << r);
+            op.cm_thr = op.cmask & ~regmask & ~1u;
+            // controls on lane bits make the selection differ between the lanes of a warp: take the
+            // branch-free form of the controlled variants there
+            const uint32_t lanemask = 0xEu | (1u << ph.lane_bits[0]) | (1u << ph.lane_bits[1]);
+            if (op.cm_thr & lanemask) {
+                if (op.variant == QSV_V_CTRL_DENSE) op.variant = QSV_V_CTRL_DENSE_SEL;
+                else if (op.variant == QSV_V_CTRL_DIAG1) op.variant = QSV_V_CTRL_DIAG1_SEL;
+                else if (op.variant == QSV_V_CTRL_SWAP) op.variant = QSV_V_CTRL_SWAP_SEL;
             }
         }
         nph++;
@@ -238,6 +319,9 @@ int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
         layout_for_kw(s.kw, &rb, &wb);
         w.push_back(s.kw); w.push_back(s.lo); w.push_back(s.nh);
         for (int i = 0; i < QSV_KW_MAX; i++) w.push_back(i < s.nh ? s.H[i] : -1);
+        w.push_back(s.tma_rank);
+        for (int d = 0; d < QSV_TMA_MAX_RANK; d++) w.push_back(d < s.tma_rank ? s.tdim_free[d] : -1);
+        for (int d = 0; d < QSV_TMA_MAX_RANK; d++) w.push_back(d < s.tma_rank ? s.tdim_box[d] : -1);
         w.push_back(s.nphases); w.push_back(s.nops);
         for (int p = 0; p < s.nphases; p++) {
             const QsvPhase &ph = s.phases[p];
@@ -250,6 +334,8 @@ int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
             const QsvOp &op = s.ops[o];
             w.push_back(op.tbit); w.push_back(op.slot); w.push_back((int32_t)op.cmask);
             w.push_back(op.cls0); w.push_back(op.cls1);
+            w.push_back(op.kind); w.push_back(op.cls); w.push_back(op.cm_reg); w.push_back(op.cm_c);
+            w.push_back((int32_t)op.cm_thr); w.push_back(op.variant);
             int32_t b[8];
             std::memcpy(b, op.m0, 32);
             for (int e = 0; e < 8; e++) w.push_back(b[e]);

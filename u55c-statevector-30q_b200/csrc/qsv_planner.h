@@ -31,6 +31,10 @@ struct PhysPass {
 int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPass> &out, std::string &err);
 // Register/warp bit split of the consumer layout for a window of kw qubits (kw in 10..13).
 int layout_for_kw(int kw, int *rb, int *wb);
+// Choose the 13-qubit layout: 4 register bits x 8 consumer warps, or 3 x 16 (process-wide).
+int set_rb13(int rb);
+// How many of a phase's targets (tile bits >= 4) may sit on lane bits 3, 4 (0..2; default 2).
+int set_phase_lanes(int k);
 // Merge consecutive passes into sweeps of window kw; merged windows keep >= 2^lo_merge contiguous amps.
 int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,
                  std::string &err);

@@ -57,6 +57,8 @@ def load(path=LIB_PATH):
         "qsv_device_status": ([P], I32),
         "qsv_take_launch_count": ([], ctypes.c_longlong),
         "qsv_set_lo_merge": ([ctypes.c_int], I32),
+        "qsv_set_layout13": ([ctypes.c_int], I32),
+        "qsv_set_phase_lanes": ([ctypes.c_int], I32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -70,7 +72,8 @@ def exported_symbols():
     """Names of the C ABI functions declared in include/qsv_b200.h."""
     return ["qsv_version", "qsv_last_error", "qsv_run_segment", "qsv_remap", "qsv_zero_state",
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_chunk_probs_f64", "qsv_sample_f64",
-            "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge"]
+            "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
+            "qsv_set_layout13", "qsv_set_phase_lanes"]
 
 
 def _check(rc):
@@ -188,7 +191,6 @@ def plan_segment(seg, n):
 
 
 def _parse_plan(w, n):
-    rb_of = {13: 4, 12: 4, 11: 3, 10: 2}
     pos = 1
     sweeps = []
     for _ in range(int(w[0])):
@@ -196,21 +198,27 @@ def _parse_plan(w, n):
         pos += 3
         H = [int(x) for x in w[pos:pos + 13] if x >= 0]
         pos += 13
+        rank = int(w[pos])
+        tfree = [int(x) for x in w[pos + 1:pos + 1 + rank]]
+        tbox = [int(x) for x in w[pos + 6:pos + 6 + rank]]
+        pos += 11
         nph, nops = int(w[pos]), int(w[pos + 1])
         pos += 2
         phases = []
         for _ in range(nph):
-            rec = [int(x) for x in w[pos:pos + 11]]
-            pos += 11
-            phases.append(dict(reg_bits=[r for r in rec[:4] if r >= 0][:rb_of[kw]], lane_bits=rec[4:6],
-                               warp_bits=[r for r in rec[6:9] if r >= 0], op_begin=rec[9], op_end=rec[10]))
+            rec = [int(x) for x in w[pos:pos + 12]]
+            pos += 12
+            phases.append(dict(reg_bits=[r for r in rec[:4] if r >= 0], lane_bits=rec[4:6],
+                               warp_bits=[r for r in rec[6:10] if r >= 0], op_begin=rec[10], op_end=rec[11]))
         ops = []
         for _ in range(nops):
-            tbit, slot, cmask, c0, c1 = (int(x) for x in w[pos:pos + 5])
-            m = w[pos + 5:pos + 21].view(np.float32).copy()
-            pos += 21
-            ops.append(dict(tbit=tbit, slot=slot, cmask=cmask & 0xFFFFFFFF, cls0=c0, cls1=c1, m0=m[:8], m1=m[8:]))
-        sweeps.append(dict(kw=kw, lo=lo, H=H, window=list(range(lo)) + H, phases=phases, ops=ops))
+            tbit, slot, cmask, c0, c1, kind, cls, cm_reg, cm_c, cm_thr, variant = (int(x) for x in w[pos:pos + 11])
+            m = w[pos + 11:pos + 27].view(np.float32).copy()
+            pos += 27
+            ops.append(dict(tbit=tbit, slot=slot, cmask=cmask & 0xFFFFFFFF, cls0=c0, cls1=c1, kind=kind, cls=cls,
+                            cm_reg=cm_reg, cm_c=cm_c, cm_thr=cm_thr & 0xFFFFFFFF, variant=variant, m0=m[:8], m1=m[8:]))
+        sweeps.append(dict(kw=kw, lo=lo, H=H, window=list(range(lo)) + H, phases=phases, ops=ops,
+                           tma_rank=rank, tdim_free=tfree, tdim_box=tbox))
     return sweeps
 
 
@@ -226,3 +234,11 @@ def take_launch_count():
 
 def set_lo_merge(lo):
     _check(load().qsv_set_lo_merge(int(lo)))
+
+
+def set_layout13(rb):
+    _check(load().qsv_set_layout13(int(rb)))
+
+
+def set_phase_lanes(k):
+    _check(load().qsv_set_phase_lanes(int(k)))
