@@ -9,6 +9,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstring>
+#include <mutex>
+
 #include "qsv_device.cuh"
 
 namespace qsv {
@@ -306,6 +309,46 @@ cudaError_t launch_reduce(const float2 *state, int n, double *out, void *scratch
     if (e != cudaSuccess) return e;
     dev::reduce_final_kernel<<<1, 64, 0, stream>>>(partials, nblocks, B, n, out);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- reduction without caller scratch
+// Fixed-size scratch for reduce_f64_noalloc: every supported state (n <= 34) needs at most
+// 2^(n-B) * (B+1) <= 1024 * 26 doubles of block partials; the array holds 32768 doubles (256 KiB). It is
+// part of the module image, so every GPU that loads the library keeps it until the process exits.
+#define QSV_NOALLOC_REDUCE_DOUBLES 32768
+static __device__ __align__(256) double g_noalloc_reduce_scratch[QSV_NOALLOC_REDUCE_DOUBLES];
+
+size_t noalloc_reduce_capacity() { return QSV_NOALLOC_REDUCE_DOUBLES * sizeof(double); }
+
+// Device address of the fixed scratch for the current device. Looked up once per device (the host-side
+// name of the array is only a stand-in for it, never a device address).
+static cudaError_t noalloc_scratch_ptr(double **out) {
+    static std::mutex mu;
+    static double *ptr[64] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_reduce_scratch);
+        if (e != cudaSuccess) return e;
+        ptr[dev] = static_cast<double *>(p);
+    }
+    *out = ptr[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need) {
+    const int B = reduce_bits(n);
+    const size_t doubles = ((size_t)1 << (n - B)) * (B + 1);
+    *need = doubles * sizeof(double);
+    if (doubles > QSV_NOALLOC_REDUCE_DOUBLES) return cudaErrorInvalidValue;
+    double *scratch = nullptr;
+    cudaError_t e = noalloc_scratch_ptr(&scratch);
+    if (e != cudaSuccess) return e;
+    return launch_reduce(state, n, out, scratch, stream);
 }
 
 cudaError_t launch_chunk_probs(const float2 *state, int n, int cb, double *out, cudaStream_t stream) {

@@ -19,6 +19,8 @@ cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni,
                           void *scratch, cudaStream_t stream);
 size_t reduce_scratch_bytes(int n, int chunk_bits);
 cudaError_t take_device_status(int *out);
+cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need);
+size_t noalloc_reduce_capacity();
 }  // namespace qsv
 
 static thread_local std::string t_err;
@@ -148,6 +150,21 @@ int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *s
     if (scratch_bytes < qsv_reduce_scratch_bytes(n)) return fail(QSV_ERR_SCRATCH, "scratch too small");
     cudaError_t e = qsv::launch_reduce((const float2 *)state, n, out_dev, scratch, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "reduce launch");
+    t_launches += 2;
+    return QSV_OK;
+}
+
+int qsv_reduce_f64_noalloc(const void *state, int n, int dtype, double *out_dev, void *stream) {
+    if (!state || !out_dev) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (n < QSV_N_MIN || n > QSV_N_MAX)
+        return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34] for the fixed-scratch reduction");
+    size_t need = 0;
+    cudaError_t e = qsv::launch_reduce_noalloc((const float2 *)state, n, out_dev, (cudaStream_t)stream, &need);
+    if (need > qsv::noalloc_reduce_capacity())
+        return fail(QSV_ERR_SCRATCH, "state needs " + std::to_string(need) + " B of block partials, fixed scratch holds " +
+                                         std::to_string(qsv::noalloc_reduce_capacity()) + " B");
+    if (e != cudaSuccess) return cuda_fail(e, "fixed-scratch reduce");
     t_launches += 2;
     return QSV_OK;
 }

@@ -51,6 +51,7 @@ def load(path=LIB_PATH):
         "qsv_zero_state": ([P, ctypes.c_int, ctypes.c_int, P], I32),
         "qsv_reduce_scratch_bytes": ([ctypes.c_int], SZ),
         "qsv_reduce_f64": ([P, ctypes.c_int, ctypes.c_int, P, P, SZ, P], I32),
+        "qsv_reduce_f64_noalloc": ([P, ctypes.c_int, ctypes.c_int, P, P], I32),
         "qsv_chunk_probs_f64": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P], I32),
         "qsv_sample_f64": ([P, ctypes.c_int, ctypes.c_int, P, ctypes.c_int, P, P, SZ, P], I32),
         "qsv_plan_segment": ([P, SZ, ctypes.c_int, P, SZ], I32),
@@ -71,7 +72,8 @@ def load(path=LIB_PATH):
 def exported_symbols():
     """Names of the C ABI functions declared in include/qsv_b200.h."""
     return ["qsv_version", "qsv_last_error", "qsv_run_segment", "qsv_remap", "qsv_zero_state",
-            "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_chunk_probs_f64", "qsv_sample_f64",
+            "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
+            "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
             "qsv_set_layout13", "qsv_set_phase_lanes"]
 
