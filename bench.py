@@ -34,6 +34,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "u55c-statevector-30q_b200")
 METRIC = "30q pass sweep GB/s (random-layer d24)"
 HBM_FALLBACK_GBS = 6650.0
+# dram__bytes_read.sum + dram__bytes_write.sum per sweep launch over the algorithmic 16 B x 2^n, measured
+# with ncu on the 26-qubit version of this workload (72 launches, median); traffic grows as 2^n
+TRAFFIC_PER_ALGORITHMIC = 0.943
 
 
 def _package():
@@ -284,7 +287,8 @@ def main():
                "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 arithmetic)",
                "data": "synthetic (seeded random-layer circuit)", "config": cfg,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                            "frac": achieved / peak, "peak_kind": peak_kind,
+                            "traffic": TRAFFIC_PER_ALGORITHMIC * bytes_per_sweep,
                             "kernel": "qsv::dev::sweep_kernel<13,4,3,3>",
                             "algorithmic_bytes_per_launch": bytes_per_sweep},
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
