@@ -101,6 +101,23 @@ QSV_API int qsv_chunk_probs_f64(const void *state, int n, int dtype, int chunk_b
 QSV_API int qsv_sample_f64(const void *state, int n, int dtype, const double *uniforms_dev, int shots, int64_t *out_dev,
                    void *scratch, size_t scratch_bytes, void *stream);
 
+/* ---------------------------------------------------------------- batched execution
+ * Many small circuits per launch (no reference counterpart: the reference runs one circuit per launch,
+ * paper/revised/sections/discussion.tex:8 lists batching as future work). A circuit of n in [10, 13] qubits
+ * is one tile: its whole program runs inside one CTA's shared memory, one HBM read and one write per
+ * circuit. Build on the host (qsv_batch_new / qsv_batch_add, one call per circuit with all its QSV2
+ * segments, L = n each), copy the tables once into a caller-provided device workspace (qsv_batch_upload),
+ * then qsv_batch_launch runs every circuit in place on its state (one kernel launch per qubit count
+ * present; capturable in a CUDA graph and replayable as long as the states and the workspace stay). */
+typedef struct qsv_batch qsv_batch;
+QSV_API qsv_batch *qsv_batch_new(void);
+QSV_API void qsv_batch_free(qsv_batch *batch);
+QSV_API int qsv_batch_add(qsv_batch *batch, void *state, int n, int nseg, const int32_t *const *segs,
+                          const size_t *nwords);
+QSV_API size_t qsv_batch_workspace_bytes(qsv_batch *batch);
+QSV_API int qsv_batch_upload(qsv_batch *batch, void *workspace, size_t bytes, void *stream);
+QSV_API int qsv_batch_launch(qsv_batch *batch, void *workspace, size_t bytes, void *stream);
+
 /* Host-side decode of a segment into the sweep plan the engine launches, for inspection and tests.
  * Writes at most `cap` int32 words to `out` (layout in csrc/qsv_plan.h, qsv_plan_serialize) and returns
  * the number of words of the full plan, or a negative error code. Pure host code, no device work. */

@@ -12,8 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqsv_b200.so")
-SOURCES = ["qsv_capi.cu", "qsv_sweep.cu", "qsv_aux.cu", "qsv_planner.cpp"]
-HEADERS = ["qsv_plan.h", "qsv_planner.h", "qsv_device.cuh"]
+SOURCES = ["qsv_capi.cu", "qsv_sweep.cu", "qsv_aux.cu", "qsv_batch.cu", "qsv_planner.cpp"]
+HEADERS = ["qsv_plan.h", "qsv_planner.h", "qsv_device.cuh", "qsv_ops.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -3,6 +3,7 @@
 
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,13 @@ cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni,
                           void *scratch, cudaStream_t stream);
 size_t reduce_scratch_bytes(int n, int chunk_bits);
 cudaError_t take_device_status(int *out);
+struct Batch;
+Batch *batch_new();
+void batch_free(Batch *b);
+int batch_add(Batch *b, void *state, int n, int nseg, const int32_t *const *segs, const size_t *nwords, std::string &err);
+size_t batch_workspace_bytes(Batch *b);
+cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
+cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
 cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
 }  // namespace qsv
@@ -199,6 +207,52 @@ int qsv_device_status(int *status) {
     cudaError_t e = qsv::take_device_status(&v);
     if (e != cudaSuccess) return cuda_fail(e, "device status");
     *status = v;
+    return QSV_OK;
+}
+
+struct qsv_batch {
+    qsv::Batch *impl;
+};
+
+qsv_batch *qsv_batch_new(void) {
+    qsv_batch *b = new (std::nothrow) qsv_batch;
+    if (!b) { fail(QSV_ERR_INVALID_ARG, "out of host memory"); return nullptr; }
+    b->impl = qsv::batch_new();
+    return b;
+}
+
+void qsv_batch_free(qsv_batch *b) {
+    if (!b) return;
+    qsv::batch_free(b->impl);
+    delete b;
+}
+
+int qsv_batch_add(qsv_batch *b, void *state, int n, int nseg, const int32_t *const *segs, const size_t *nwords) {
+    if (!b || !state || (nseg > 0 && (!segs || !nwords)) || nseg < 0) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    std::string err;
+    int rc = qsv::batch_add(b->impl, state, n, nseg, segs, nwords, err);
+    if (rc) return fail(rc, err);
+    return QSV_OK;
+}
+
+size_t qsv_batch_workspace_bytes(qsv_batch *b) { return b ? qsv::batch_workspace_bytes(b->impl) : 0; }
+
+int qsv_batch_upload(qsv_batch *b, void *workspace, size_t bytes, void *stream) {
+    if (!b || !workspace) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (bytes < qsv::batch_workspace_bytes(b->impl)) return fail(QSV_ERR_SCRATCH, "batch workspace too small");
+    cudaError_t e = qsv::batch_upload(b->impl, workspace, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch upload");
+    return QSV_OK;
+}
+
+int qsv_batch_launch(qsv_batch *b, void *workspace, size_t bytes, void *stream) {
+    if (!b || !workspace) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (bytes < qsv::batch_workspace_bytes(b->impl)) return fail(QSV_ERR_SCRATCH, "batch workspace too small");
+    int launches = 0;
+    std::lock_guard<std::mutex> lk(g_launch_mu);
+    cudaError_t e = qsv::batch_launch(b->impl, workspace, sm_count(), (cudaStream_t)stream, &launches);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    t_launches += launches;
     return QSV_OK;
 }
 

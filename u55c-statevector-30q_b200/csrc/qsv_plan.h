@@ -92,6 +92,15 @@ struct QsvPhase {
     uint8_t pad[4];
 };
 
+// phase with 32-bit op indices (whole-circuit programs of the batch kernel can exceed 255 ops)
+struct QsvPhaseX {
+    uint8_t reg_bits[QSV_RB_MAX];
+    uint8_t lane_bits[2];
+    uint8_t warp_bits[QSV_WB_MAX];
+    uint8_t pad[2];
+    int32_t op_begin, op_end;
+};
+
 struct QsvSweep {
     int32_t n;                  // state qubits
     int32_t kw;                 // window size (tile = 2^kw amplitudes)

@@ -133,28 +133,17 @@ static int tma_dims(const QsvSweep &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *
     return rank;
 }
 
-static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
-                      QsvSweep &sw, std::string &err) {
+// Ops [b, e) in tile coordinates of a window (tile_of[q] = tile bit of physical qubit q) and their phases.
+// Phases are greedy in op order: tile bits >= 4 that are targets need a register or lane slot.
+static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n, int kw,
+                       std::vector<QsvOp> &out, std::vector<QsvPhaseX> &phases, std::string &err) {
     int rb, wb;
     if (layout_for_kw(kw, &rb, &wb)) { err = "unsupported window size"; return QSV_ERR_UNSUPPORTED; }
-    std::memset(&sw, 0, sizeof(sw));
-    const int lo = window_lo(qset, n, kw);
-    if (lo < QSV_LO_MIN) { err = "op qubits do not fit one 13-qubit window"; return QSV_ERR_UNSUPPORTED; }
-    sw.n = n;
-    sw.kw = kw;
-    sw.lo = lo;
-    int tile_of[64];
-    for (int q = 0; q < 64; q++) tile_of[q] = -1;
-    for (int q = 0; q < lo; q++) tile_of[q] = q;
-    int nh = 0;
-    for (int q = lo; q < n; q++)
-        if ((qset >> q) & 1) { sw.H[nh] = (uint8_t)q; tile_of[q] = lo + nh; nh++; }
-    sw.nh = nh;
-    sw.ntiles = 1ll << (n - kw);
-    sw.nops = (int)(e - b);
-    // ops in tile coordinates
+    out.assign(e - b, QsvOp());
+    phases.clear();
     for (size_t i = b; i < e; i++) {
-        QsvOp &o = sw.ops[i - b];
+        QsvOp &o = out[i - b];
+        std::memset(&o, 0, sizeof(o));
         const PhysOp &p = ops[i];
         std::memcpy(o.m0, p.m0, sizeof(o.m0));
         std::memcpy(o.m1, p.m1, sizeof(o.m1));
@@ -188,22 +177,14 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
             o.variant = QSV_V_MUX;
         }
     }
-    {
-        uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
-        const int r = tma_dims(sw, tfree, tbox, tstart);
-        sw.tma_rank = (uint8_t)r;
-        for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
-    }
-    // phases: greedy in op order; tile bits >= 4 that are targets need a register or lane slot
     const int cap = rb + g_phase_lanes;
-    int nph = 0;
+    const size_t nops = out.size();
     size_t i = 0;
-    while (i < (size_t)sw.nops) {
-        if (nph >= QSV_MAX_PHASES) { err = "too many phases"; return QSV_ERR_UNSUPPORTED; }
+    while (i < nops) {
         size_t j = i;
         int used[QSV_KW_MAX], cnt[QSV_KW_MAX], nu = 0;
-        while (j < (size_t)sw.nops) {
-            const int tb = sw.ops[j].tbit;
+        while (j < nops) {
+            const int tb = out[j].tbit;
             if (tb >= 4) {
                 int f = -1;
                 for (int u = 0; u < nu; u++)
@@ -219,10 +200,11 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         // order targets by use count (stable): most used go to register bits
         int order[QSV_KW_MAX];
         for (int u = 0; u < nu; u++) order[u] = u;
-        std::stable_sort(order, order + nu, [&](int a, int c) { return cnt[a] > cnt[c]; });
-        QsvPhase &ph = sw.phases[nph];
+        std::stable_sort(order, order + nu, [&](int x, int y) { return cnt[x] > cnt[y]; });
+        QsvPhaseX ph;
+        std::memset(&ph, 0, sizeof(ph));
         bool taken[QSV_KW_MAX] = {false};
-        int slots[QSV_KW_MAX], ns = 0;   // reg bits then lane bits 3, 4 then warp bits
+        int slots[QSV_KW_MAX], ns = 0;
         for (int u = 0; u < nu; u++) { slots[ns++] = used[order[u]]; taken[used[order[u]]] = true; }
         // targets beyond rb go to lane slots; unused reg/lane slots and warp slots get the remaining bits
         int regs[QSV_RB_MAX], nr = 0, lanes[2], nl = 0;
@@ -240,12 +222,12 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         for (int r = 0; r < rb; r++) ph.reg_bits[r] = (uint8_t)regs[r];
         ph.lane_bits[0] = (uint8_t)lanes[0];
         ph.lane_bits[1] = (uint8_t)lanes[1];
-        ph.op_begin = (uint8_t)i;
-        ph.op_end = (uint8_t)j;
+        ph.op_begin = (int32_t)i;
+        ph.op_end = (int32_t)j;
         uint32_t regmask = 0;
         for (int r = 0; r < rb; r++) regmask |= 1u << ph.reg_bits[r];
         for (size_t o = i; o < j; o++) {
-            QsvOp &op = sw.ops[o];
+            QsvOp &op = out[o];
             const int tb = op.tbit;
             if (tb == 0) op.slot = QSV_SLOT_COMP;
             else if (tb < 4) op.slot = (uint8_t)(QSV_SLOT_LANE0 + tb - 1);
@@ -271,11 +253,63 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
                 else if (op.variant == QSV_V_CTRL_SWAP) op.variant = QSV_V_CTRL_SWAP_SEL;
             }
         }
-        nph++;
+        phases.push_back(ph);
         i = j;
     }
-    sw.nphases = nph;
     return QSV_OK;
+}
+
+static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
+                      QsvSweep &sw, std::string &err) {
+    int rb, wb;
+    if (layout_for_kw(kw, &rb, &wb)) { err = "unsupported window size"; return QSV_ERR_UNSUPPORTED; }
+    std::memset(&sw, 0, sizeof(sw));
+    const int lo = window_lo(qset, n, kw);
+    if (lo < QSV_LO_MIN) { err = "op qubits do not fit one 13-qubit window"; return QSV_ERR_UNSUPPORTED; }
+    sw.n = n;
+    sw.kw = kw;
+    sw.lo = lo;
+    int tile_of[64];
+    for (int q = 0; q < 64; q++) tile_of[q] = -1;
+    for (int q = 0; q < lo; q++) tile_of[q] = q;
+    int nh = 0;
+    for (int q = lo; q < n; q++)
+        if ((qset >> q) & 1) { sw.H[nh] = (uint8_t)q; tile_of[q] = lo + nh; nh++; }
+    sw.nh = nh;
+    sw.ntiles = 1ll << (n - kw);
+    {
+        uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
+        const int r = tma_dims(sw, tfree, tbox, tstart);
+        sw.tma_rank = (uint8_t)r;
+        for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
+    }
+    std::vector<QsvOp> vops;
+    std::vector<QsvPhaseX> vph;
+    int rc = plan_window(ops, b, e, tile_of, n, kw, vops, vph, err);
+    if (rc) return rc;
+    if (vops.size() > QSV_MAX_SWEEP_OPS || vph.size() > QSV_MAX_PHASES) { err = "sweep too large"; return QSV_ERR_UNSUPPORTED; }
+    sw.nops = (int)vops.size();
+    sw.nphases = (int)vph.size();
+    std::memcpy(sw.ops, vops.data(), vops.size() * sizeof(QsvOp));
+    for (size_t p = 0; p < vph.size(); p++) {
+        QsvPhase &d = sw.phases[p];
+        const QsvPhaseX &x = vph[p];
+        std::memcpy(d.reg_bits, x.reg_bits, sizeof(d.reg_bits));
+        std::memcpy(d.lane_bits, x.lane_bits, sizeof(d.lane_bits));
+        std::memcpy(d.warp_bits, x.warp_bits, sizeof(d.warp_bits));
+        d.op_begin = (uint8_t)x.op_begin;
+        d.op_end = (uint8_t)x.op_end;
+    }
+    return QSV_OK;
+}
+
+int plan_whole_state(const std::vector<PhysPass> &passes, int n, std::vector<QsvOp> &ops_out,
+                     std::vector<QsvPhaseX> &phases_out, std::string &err) {
+    std::vector<PhysOp> ops;
+    for (const PhysPass &p : passes) ops.insert(ops.end(), p.ops.begin(), p.ops.end());
+    int tile_of[64];
+    for (int q = 0; q < 64; q++) tile_of[q] = q < n ? q : -1;
+    return plan_window(ops, 0, ops.size(), tile_of, n, n, ops_out, phases_out, err);
 }
 
 int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,

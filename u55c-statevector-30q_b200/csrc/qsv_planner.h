@@ -38,6 +38,10 @@ int set_phase_lanes(int k);
 // Merge consecutive passes into sweeps of window kw; merged windows keep >= 2^lo_merge contiguous amps.
 int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,
                  std::string &err);
+// Whole-state program of an n-qubit circuit (n in 10..13: the state is one tile): every op of every pass,
+// in order, with its phases.
+int plan_whole_state(const std::vector<PhysPass> &passes, int n, std::vector<QsvOp> &ops_out,
+                     std::vector<QsvPhaseX> &phases_out, std::string &err);
 // Flatten a plan into int32 words (layout documented in qsv_b200.h / the planner tests).
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap);
 

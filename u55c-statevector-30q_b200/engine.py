@@ -59,6 +59,12 @@ def load(path=LIB_PATH):
         "qsv_take_launch_count": ([], ctypes.c_longlong),
         "qsv_set_lo_merge": ([ctypes.c_int], I32),
         "qsv_set_layout13": ([ctypes.c_int], I32),
+        "qsv_batch_new": ([], P),
+        "qsv_batch_free": ([P], None),
+        "qsv_batch_add": ([P, P, ctypes.c_int, ctypes.c_int, P, P], I32),
+        "qsv_batch_workspace_bytes": ([P], SZ),
+        "qsv_batch_upload": ([P, P, SZ, P], I32),
+        "qsv_batch_launch": ([P, P, SZ, P], I32),
         "qsv_set_phase_lanes": ([ctypes.c_int], I32),
     }
     for name, (args, res) in sig.items():
@@ -75,7 +81,8 @@ def exported_symbols():
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
             "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
-            "qsv_set_layout13", "qsv_set_phase_lanes"]
+            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
+            "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch"]
 
 
 def _check(rc):
@@ -222,6 +229,49 @@ def _parse_plan(w, n):
         sweeps.append(dict(kw=kw, lo=lo, H=H, window=list(range(lo)) + H, phases=phases, ops=ops,
                            tma_rank=rank, tdim_free=tfree, tdim_box=tbox))
     return sweeps
+
+
+class SmallBatch:
+    """Whole-circuit batch for circuits of 10..13 qubits (qsv_batch_* in the C ABI): each circuit's entire
+    program runs inside one CTA's shared memory. Add circuits (state tensor + QSV2 segments), upload the
+    tables once into a device workspace, then launch (capturable in a CUDA graph, replayable)."""
+
+    def __init__(self):
+        self._lib = load()
+        self._h = self._lib.qsv_batch_new()
+        if not self._h:
+            raise QSVError(-1, self._lib.qsv_last_error().decode())
+        self.workspace = None
+        self.count = 0
+        self._keep = []
+
+    def add(self, state, segments):
+        n = _qubits(state)
+        words = [np.ascontiguousarray(s, dtype=np.int32) for s in segments]
+        ptrs = (ctypes.c_void_p * len(words))(*[w.ctypes.data for w in words])
+        sizes = (ctypes.c_size_t * len(words))(*[w.size for w in words])
+        _check(self._lib.qsv_batch_add(self._h, _ptr(state), n, len(words), ptrs, sizes))
+        self._keep.append(state)
+        self.count += 1
+
+    def upload(self, stream=None):
+        torch = _torch()
+        nbytes = int(self._lib.qsv_batch_workspace_bytes(self._h))
+        self.workspace = torch.empty(max(nbytes, 256), dtype=torch.uint8, device="cuda")
+        _check(self._lib.qsv_batch_upload(self._h, _ptr(self.workspace), self.workspace.numel(), _stream(stream)))
+
+    def launch(self, stream=None):
+        if self.workspace is None:
+            self.upload(stream)
+        _check(self._lib.qsv_batch_launch(self._h, _ptr(self.workspace), self.workspace.numel(), _stream(stream)))
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.qsv_batch_free(self._h)
+                self._h = None
+        except Exception:
+            pass
 
 
 def device_status():
