@@ -61,19 +61,27 @@ def _count(d, key, inc=1):
     d[key] = d.get(key, 0) + inc
 
 
+def _close_to_identity(R):
+    """np.allclose(R, I, atol=1e-12) (rtol 1e-5): off-diagonal |R_ij| <= 1e-12, |R_ii - 1| <= 1e-12 + 1e-5."""
+    d = np.diagonal(R)
+    if np.any(np.abs(d - 1.0) > 1e-12 + 1e-5):
+        return False
+    off = R - np.diag(d)
+    return not np.any(np.abs(off) > 1e-12)
+
+
 def controlled_target(M, nq):
     """If M (2^nq, Qiskit order) is a 2x2 on one gate qubit j controlled by all the others being 1,
     return (j, U); else None (compiler.py:63-75)."""
     full = (1 << nq) - 1
-    eye = np.eye(1 << nq)
     for j in range(nq):
         i1 = full
         i0 = full & ~(1 << j)
         sel = [i0, i1]
         U = M[np.ix_(sel, sel)].copy()
-        rest = M.copy()
+        rest = np.array(M, dtype=complex)
         rest[np.ix_(sel, sel)] = I2
-        if np.allclose(rest, eye, atol=1e-12):
+        if _close_to_identity(rest):
             return j, U
     return None
 
@@ -82,8 +90,8 @@ def ops_2q(M, a, b, stats):
     """4x4 gate on storage qubits (a, b), basis bit_a + 2*bit_b -> MUX2 ops (compiler.py:78-92):
     diagonal -> one MUX2 on b selected by a; controlled-U -> one MUX2; otherwise the cosine-sine
     decomposition into three MUX2 (block-diag on a | rotation on b | block-diag on a)."""
-    if np.allclose(M, np.diag(np.diag(M)), atol=1e-12):
-        d = np.diag(M)
+    d = np.diag(M)
+    if not np.any(np.abs(M - np.diag(d)) > 1e-12):      # np.allclose(M, diag(M), atol=1e-12)
         return [Op(b, (a,), np.diag([d[0], d[2]]), np.diag([d[1], d[3]]))]
     ct = controlled_target(M, 2)
     if ct is not None:
@@ -192,8 +200,9 @@ def circuit_to_ops(qc, stats, fuse_1q=True, max_width=None):
 def pass_window(qubits, k, max_high=MAX_HIGH):
     """Smallest m in 0..max_high such that at most m of `qubits` lie at or above k - m; returns
     (m, sorted high qubits), or None when no m fits (compiler.py:176-183)."""
+    qs = sorted(q for q in qubits if q >= k - max_high)
     for m in range(max_high + 1):
-        hi = sorted(q for q in qubits if q >= k - m)
+        hi = [q for q in qs if q >= k - m]
         if len(hi) <= m:
             return m, hi
     return None
@@ -290,17 +299,23 @@ def encode_segment(passes, L, k, M=MAX_HIGH):
         for i, q in enumerate(hi):
             tile_of[q] = k - m + i
         words += [m, slots[0], slots[1], len(p), slots[2], slots[3], 0, 0]
-        for op, ph in p:
+        # op records: matrices rounded to complex64 together (same per-entry rounding as one by one)
+        mats = np.empty((len(p), 2, 4), dtype=np.complex128)
+        for j, (op, ph) in enumerate(p):
+            mats[j, 0] = np.asarray(op.M0, dtype=complex).reshape(-1)
+            mats[j, 1] = np.asarray(op.M1, dtype=complex).reshape(-1)
+        c64 = mats.astype(np.complex64)
+        fl = np.empty((len(p), 16), dtype=np.float32)
+        fl[:, 0:8:2], fl[:, 1:8:2] = c64[:, 0].real, c64[:, 0].imag
+        fl[:, 8:16:2], fl[:, 9:16:2] = c64[:, 1].real, c64[:, 1].imag
+        fbits = fl.view(np.int32)
+        for j, (op, ph) in enumerate(p):
             tq = [tile_of[q] for q in ph]
             cmask = 0
             for c in tq[1:]:
                 cmask |= 1 << c
-            f = np.zeros(16, dtype=np.float32)
-            for i, mat in enumerate((op.M0, op.M1)):
-                c64 = np.asarray(mat, dtype=np.complex64).reshape(-1)
-                f[8 * i:8 * i + 8:2] = c64.real
-                f[8 * i + 1:8 * i + 8:2] = c64.imag
-            words += [OP_MUX2, tq[0], cmask, 0, 0, 0, 0, 0] + list(f.view(np.int32))
+            words += [OP_MUX2, tq[0], cmask, 0, 0, 0, 0, 0]
+            words += fbits[j].tolist()
     arr = np.asarray(words, dtype=np.int64)
     return (arr & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
 

@@ -112,32 +112,45 @@ _ONE = {
 }
 
 
+def _const(M):
+    M = np.array(M, dtype=complex)
+    M.setflags(write=False)
+    return M
+
+
+# parameterless multi-qubit gates: built once (read-only; callers never modify gate matrices)
+_FIXED = {
+    "cx": _const(controlled(X)), "cy": _const(controlled(Y)), "cz": _const(controlled(Z)),
+    "ch": _const(controlled(H)), "csx": _const(controlled(SX)), "cs": _const(controlled(S)),
+    "csdg": _const(controlled(SDG)), "swap": _const(SWAP), "iswap": _const(ISWAP), "ecr": _const(ECR),
+    "dcx": _const(DCX), "ccx": _const(controlled(X, 2)), "ccz": _const(controlled(Z, 2)),
+    "cswap": _const(cswap()), "c3x": _const(controlled(X, 3)), "c4x": _const(controlled(X, 4)),
+}
+_XX, _YY, _ZZ, _ZX = _kron_le(X, X), _kron_le(Y, Y), _kron_le(Z, Z), _kron_le(Z, X)
+# parameterised multi-qubit gates: name -> builder(params)
+_PARAM = {
+    "cp": lambda p: controlled(phase(p[0])), "cu1": lambda p: controlled(phase(p[0])),
+    "crx": lambda p: controlled(rx(p[0])), "cry": lambda p: controlled(ry(p[0])),
+    "crz": lambda p: controlled(rz(p[0])),
+    "cu": lambda p: controlled(cmath.exp(1j * p[3]) * u3(p[0], p[1], p[2])),
+    "cu3": lambda p: controlled(u3(p[0], p[1], p[2])),
+    "rxx": lambda p: _expm_herm(_XX, p[0]), "ryy": lambda p: _expm_herm(_YY, p[0]),
+    "rzz": lambda p: _expm_herm(_ZZ, p[0]), "rzx": lambda p: _expm_herm(_ZX, p[0]),
+    "xx_plus_yy": lambda p: xx_plus_yy(p[0], p[1] if len(p) > 1 else 0.0),
+}
+
+
 def gate_matrix(name, params=()):
     """Dense Qiskit-convention matrix of a named gate (1q, 2q and the supported multi-qubit gates)."""
-    p = [float(x) for x in params]
     if name in _ONE:
         npar, f = _ONE[name]
-        return f(*p[:npar]) if npar else f()
-    two = {
-        "cx": lambda: controlled(X), "cy": lambda: controlled(Y), "cz": lambda: controlled(Z),
-        "ch": lambda: controlled(H), "csx": lambda: controlled(SX), "cs": lambda: controlled(S),
-        "csdg": lambda: controlled(SDG),
-        "cp": lambda: controlled(phase(p[0])), "cu1": lambda: controlled(phase(p[0])),
-        "crx": lambda: controlled(rx(p[0])), "cry": lambda: controlled(ry(p[0])),
-        "crz": lambda: controlled(rz(p[0])),
-        "cu": lambda: controlled(cmath.exp(1j * p[3]) * u3(p[0], p[1], p[2])),
-        "cu3": lambda: controlled(u3(p[0], p[1], p[2])),
-        "swap": lambda: SWAP, "iswap": lambda: ISWAP, "ecr": lambda: ECR, "dcx": lambda: DCX,
-        "rxx": lambda: _expm_herm(_kron_le(X, X), p[0]),
-        "ryy": lambda: _expm_herm(_kron_le(Y, Y), p[0]),
-        "rzz": lambda: _expm_herm(_kron_le(Z, Z), p[0]),
-        "rzx": lambda: _expm_herm(_kron_le(Z, X), p[0]),
-        "xx_plus_yy": lambda: xx_plus_yy(p[0], p[1] if len(p) > 1 else 0.0),
-        "ccx": lambda: controlled(X, 2), "ccz": lambda: controlled(Z, 2),
-        "cswap": cswap, "c3x": lambda: controlled(X, 3), "c4x": lambda: controlled(X, 4),
-    }
-    if name in two:
-        return two[name]()
+        return f(*[float(x) for x in params[:npar]]) if npar else f()
+    M = _FIXED.get(name)
+    if M is not None:
+        return M
+    f = _PARAM.get(name)
+    if f is not None:
+        return f([float(x) for x in params])
     raise KeyError(f"no matrix for gate {name!r}")
 
 

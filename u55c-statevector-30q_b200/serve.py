@@ -1,0 +1,317 @@
+"""Serving loop: continuous batching of circuits on one B200 under an HBM budget.
+
+No reference counterpart (the reference serves nothing; its latency study repeats one circuit,
+bench/latency_jitter.py, and reports p50/p99 of T_e2e -- the statistics kept here). Requests arrive over
+time; each is compiled on arrival (host), then admitted as soon as a device slot is free and its state
+fits in the remaining HBM budget (states stay resident on the device until the request completes).
+Admitted work overlaps on the GPU: requests of 10..13 qubits that are ready together run as one
+whole-circuit batch launch, larger ones each run their sweeps on their own stream. Completion is
+detected with CUDA events; the result (norm and <Z_q> per qubit, FP64, plus the state if asked) is read
+back and the memory released. Each request's arithmetic is independent of the others (no cross-request
+reduction, fixed op order), so a result is the same alone and in the mix.
+"""
+import heapq
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import engine
+from .batch import SMALL_MAX
+from .compiler import compile_circuit
+
+
+@dataclass
+class Request:
+    rid: int
+    circuit: object                 # a Circuit, or None to build it from `spec` on arrival
+    arrival: float                  # seconds from the start of the run
+    want_state: bool = False
+    spec: tuple = None              # (n, depth, seed) of a random-layer circuit with Toffolis
+    # filled in by the server
+    program: object = None
+    fmap: list = None
+    n: int = 0
+    admitted: float = None
+    done: float = None
+    result: object = None
+    state: object = None
+
+
+@dataclass
+class _Slot:
+    req: Request
+    stream: object
+    state: object
+    event: object
+    scratch: object
+    zout: object
+    bytes: int
+
+
+def config5_requests(count=20000, rate=50.0, seed=4, qmin=12, qmax=30, dmin=10, dmax=100):
+    """The served workload: Poisson arrivals at `rate` per second, qubit counts log-uniform in
+    [qmin, qmax], depths uniform in [dmin, dmax], random-layer recipe with CZ brickwork and Toffolis,
+    request i seeded seed + i."""
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, count)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    out = []
+    for i, t in enumerate(arrivals):
+        r = np.random.default_rng([seed, i])          # request i's shape depends on (seed, i) only
+        n = int(np.clip(np.floor(np.exp(r.uniform(math.log(qmin), math.log(qmax + 1)))), qmin, qmax))
+        d = int(r.integers(dmin, dmax + 1))
+        out.append(Request(i, None, float(t), spec=(n, d, seed + i)))
+    return out
+
+
+def _circuit(req):
+    if req.circuit is None:
+        from .generators import random_layer_ccx
+        n, d, s = req.spec
+        req.circuit = random_layer_ccx(n, d, s)
+    return req.circuit
+
+
+def _compile_request(payload):
+    """Compile one request (runs in a worker process or inline): -> (segments, final_map, n_run)."""
+    circuit, spec, k = payload
+    req = Request(-1, circuit, 0.0, spec=spec)
+    qc = _circuit(req)
+    n = qc.num_qubits
+    m = max(n, engine.N_MIN)
+    if m != n:
+        from .circuit import Circuit
+        q2 = Circuit(m)
+        q2.compose(qc, range(n), inplace=True)
+        qc = q2
+    prog, fmap, _ = compile_circuit(qc, m, m if m <= SMALL_MAX else k)
+    if any(kind != "segment" for kind, _ in prog):
+        raise ValueError("program needs remaps, not served here")
+    return [s for _, s in prog], fmap, m
+
+
+class Server:
+    def __init__(self, budget_bytes=160e9, max_inflight=16, device=None, k=12, compile_workers=0):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("Server needs a CUDA device (B200); none is available")
+        engine.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.budget = int(budget_bytes)
+        self.max_inflight = max_inflight
+        self.k = k
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(max_inflight)]
+        self.free_streams = deque(range(max_inflight))
+        self.used = 0
+        self.stats = dict(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0)
+        self.pool = None
+        if compile_workers:
+            import multiprocessing as mp
+            from .batch import _boot_code
+            self.pool = mp.get_context("spawn").Pool(compile_workers, initializer=exec, initargs=(_boot_code(),))
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.terminate()
+            self.pool = None
+
+    @staticmethod
+    def footprint(n):
+        """Device bytes a request holds while in flight: its state, reduction scratch, outputs."""
+        m = max(n, engine.N_MIN)
+        return (8 << m) + engine.scratch_bytes(m) + 8 * (m + 1)
+
+    def _compile(self, req):
+        self._finish_compile(req, _compile_request((req.circuit, req.spec, self.k)))
+
+    @staticmethod
+    def _finish_compile(req, res):
+        req.program, req.fmap, req.n = res
+        _circuit(req)
+
+    def _launch(self, reqs, now):
+        """Start a group of admitted requests: small ones as one whole-circuit batch, large ones alone."""
+        import torch
+        slots = []
+        small = [r for r in reqs if r.n <= SMALL_MAX]
+        large = [r for r in reqs if r.n > SMALL_MAX]
+        groups = ([small] if small else []) + [[r] for r in large]
+        for grp in groups:
+            si = self.free_streams.popleft()
+            st = self.streams[si]
+            # every buffer of the group is allocated on the group's stream, so the caching allocator
+            # never hands it to other work before this stream is done with it
+            with torch.cuda.stream(st):
+                states = [engine.new_state(r.n, device=self.device, zero=True, stream=st) for r in grp]
+                batch = None
+                if grp is small:
+                    batch = engine.SmallBatch()
+                    for r, s in zip(grp, states):
+                        batch.add(s, r.program)
+                    batch.upload(st)
+                    batch.launch(st)
+                    self.stats["small_batches"] += 1
+                    self.stats["small_in_batches"] += len(grp)
+                else:
+                    for seg in grp[0].program:
+                        engine.run_segment(states[0], seg, st)
+                outs = []
+                for r, s in zip(grp, states):
+                    sc = engine.new_scratch(r.n, self.device)
+                    outs.append((sc, engine.reduce_f64(s, scratch=sc, stream=st)))
+                ev = torch.cuda.Event()
+                ev.record(st)
+            for r, s, (sc, z) in zip(grp, states, outs):
+                r.admitted = now
+                slot = _Slot(r, si, s, ev, sc, z, self.footprint(r.n))
+                slot.batch = batch           # the batch tables stay alive until the group completes
+                slots.append(slot)
+        return slots
+
+    def run(self, requests, realtime=True, timeout=3600.0):
+        """Serve `requests` (sorted by arrival). Returns the list of completed requests."""
+        import torch
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        compiling = deque()
+        ready = deque()
+        inflight = []
+        done = []
+        t0 = time.perf_counter()
+        while pending or compiling or ready or inflight:
+            now = time.perf_counter() - t0
+            if now > timeout:
+                raise TimeoutError("serving run exceeded its time limit")
+            # arrivals: compiled on arrival (in the worker pool when there is one); a request joins the
+            # ready queue, in arrival order, once its program exists
+            while pending and (not realtime or pending[0].arrival <= now):
+                r = pending.popleft()
+                if r.program is not None:
+                    ready.append(r)
+                elif self.pool is None:
+                    self._compile(r)
+                    ready.append(r)
+                else:
+                    compiling.append((r, self.pool.apply_async(_compile_request, ((r.circuit, r.spec, self.k),))))
+                if self.pool is None and realtime:
+                    break                 # compile inline one at a time, keep the device fed meanwhile
+            while compiling and compiling[0][1].ready():
+                r, fut = compiling.popleft()
+                self._finish_compile(r, fut.get())
+                ready.append(r)
+            # admission: free slot and memory budget; continuous -- new work joins while old runs
+            admit = []
+            streams_left = len(self.free_streams)
+            small_group = False
+            while ready and streams_left > 0:
+                r = ready[0]
+                fp = self.footprint(r.n)
+                if self.used + fp > self.budget:
+                    if not inflight and not admit:
+                        raise MemoryError(f"request {r.rid} ({r.n} qubits) exceeds the HBM budget")
+                    break
+                ready.popleft()
+                self.used += fp
+                admit.append(r)
+                if r.n <= SMALL_MAX:
+                    if not small_group:
+                        small_group = True
+                        streams_left -= 1
+                else:
+                    streams_left -= 1
+            if admit:
+                inflight += self._launch(admit, now)
+                self.stats["admitted"] += len(admit)
+                self.stats["peak_bytes"] = max(self.stats["peak_bytes"], self.used)
+                self.stats["peak_inflight"] = max(self.stats["peak_inflight"], len(inflight))
+            # completions
+            still = []
+            finished_streams = set()
+            for sl in inflight:
+                if sl.event.query():
+                    z = sl.zout.cpu().numpy()
+                    r = sl.req
+                    r.done = time.perf_counter() - t0
+                    n_log = r.circuit.num_qubits
+                    r.result = (float(z[0]), np.array([z[1 + r.fmap[q]] for q in range(n_log)]))
+                    if r.want_state:
+                        perm = [r.fmap[q] for q in range(r.n)]
+                        dst = torch.empty_like(sl.state)
+                        engine.remap(sl.state, dst, perm)
+                        r.state = dst.cpu().numpy()[: 1 << n_log]
+                    self.used -= sl.bytes
+                    finished_streams.add(sl.stream)
+                    done.append(r)
+                else:
+                    still.append(sl)
+            inflight = still
+            live_streams = {sl.stream for sl in inflight}
+            for si in finished_streams - live_streams:
+                self.free_streams.append(si)
+            if not admit and not finished_streams:
+                # nothing to do right now: wait for the next arrival, compile or completion
+                wait = 0.0005
+                if pending and realtime and not ready and not inflight and not compiling:
+                    wait = max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0)))
+                time.sleep(wait)
+        return done
+
+
+def precompile(requests, workers=0):
+    """Compile every request ahead of time (optionally in spawned workers), to time the device side of
+    serving without host compile."""
+    payloads = [(r.circuit, r.spec, 12) for r in requests]
+    if workers:
+        import multiprocessing as mp
+        from .batch import _boot_code
+        with mp.get_context("spawn").Pool(workers, initializer=exec, initargs=(_boot_code(),)) as pool:
+            res = pool.map_async(_compile_request, payloads).get(3600)
+    else:
+        res = [_compile_request(p) for p in payloads]
+    for r, x in zip(requests, res):
+        Server._finish_compile(r, x)
+    return requests
+
+
+def plain_serve(requests, device=None):
+    """The plain sequential path: each request alone, in arrival order (a single FIFO server, no overlap;
+    requests without a program are compiled when they are served). Returns the completed requests with
+    admitted/done times on the same arrival clock."""
+    import torch
+    srv = Server(max_inflight=1, device=device)
+    pending = sorted(requests, key=lambda r: r.arrival)
+    t0 = time.perf_counter()
+    out = []
+    for r in pending:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        if r.program is None:
+            srv._compile(r)
+        r.admitted = time.perf_counter() - t0
+        st = engine.new_state(r.n, device=srv.device)
+        if r.n <= SMALL_MAX:
+            b = engine.SmallBatch()
+            b.add(st, r.program)
+            b.upload()
+            b.launch()
+        else:
+            for seg in r.program:
+                engine.run_segment(st, seg)
+        z = engine.reduce_f64(st).cpu().numpy()
+        r.done = time.perf_counter() - t0
+        n_log = r.circuit.num_qubits
+        r.result = (float(z[0]), np.array([z[1 + r.fmap[q]] for q in range(n_log)]))
+        out.append(r)
+        del st
+    torch.cuda.synchronize(srv.device)
+    return out
+
+
+def latency_stats(done):
+    lat = np.array([r.done - r.arrival for r in done])
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    return dict(count=len(done), p50_ms=float(np.percentile(lat, 50) * 1e3),
+                p99_ms=float(np.percentile(lat, 99) * 1e3), mean_ms=float(lat.mean() * 1e3),
+                circuits_per_s=len(done) / span if span > 0 else float("inf"))
