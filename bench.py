@@ -173,6 +173,8 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
+                    help="specialised sweep kernels (compiled before the warm-up unless off)")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -218,6 +220,12 @@ def main():
     engine.load()
     sweeps = sum(len(engine.plan_segment(s, a.n)) for s in segs)
     cfg["sweeps"] = sweeps
+    engine.set_jit(a.jit)
+    if a.jit != "off":
+        t0 = time.perf_counter()
+        ready = sum(engine.jit_prepare(s, a.n) for s in segs)
+        cfg["specialised_kernels"] = {"sweeps_ready": ready, "structures": engine.jit_info()["structures"],
+                                      "compile_s": round(time.perf_counter() - t0, 2)}
     stream = torch.cuda.current_stream(dev)
     state = engine.new_state(a.n, device=dev)
 
@@ -231,6 +239,7 @@ def main():
     if dist:
         dist.barrier()
     engine.take_launch_count()
+    jit0 = engine.jit_info()["jit_launches"]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -241,6 +250,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize(dev)
     launches = engine.take_launch_count()
+    jit_launches = engine.jit_info()["jit_launches"] - jit0
     sec = e0.elapsed_time(e1) / 1e3
     if dist:
         t = torch.tensor([sec], device=dev, dtype=torch.float64)
@@ -289,7 +299,9 @@ def main():
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_kind": peak_kind,
                             "traffic": TRAFFIC_PER_ALGORITHMIC * bytes_per_sweep,
-                            "kernel": "qsv::dev::sweep_kernel<13,4,3,3>",
+                            "kernel": ("qsv_sweep_jit (specialised per sweep structure)" if jit_launches == launches
+                                       else "qsv::dev::sweep_kernel<13,4,3,3>" if jit_launches == 0
+                                       else f"qsv_sweep_jit x{jit_launches} + sweep_kernel x{launches - jit_launches}"),
                             "algorithmic_bytes_per_launch": bytes_per_sweep},
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(out))

@@ -143,6 +143,28 @@ QSV_API int qsv_set_layout13(int rb);
  * shuffles) instead of starting a new phase, 0..2 (default 2). Values are identical either way. */
 QSV_API int qsv_set_phase_lanes(int k);
 
+/* Specialised sweep kernels (no reference counterpart; the reference's engine is one fixed HLS kernel).
+ * qsv_run_segment can launch, instead of the interpreter kernel, a kernel compiled at run time (NVRTC,
+ * sm_100a) for the sweep's structure: its phase layouts and, per op, target slot, code variant and control
+ * masks (everything but the matrices and the window). Values are identical either way.
+ * mode 0 = interpreter only; 1 = eager: a new structure is compiled (blocking) before its first launch;
+ * 2 = automatic (default): a structure is compiled in background threads once it has been launched twice,
+ * and used from the first launch after its kernel is ready. Returns the previous mode. Process-wide. */
+QSV_API int qsv_set_jit(int mode);
+
+/* Compile, in parallel and blocking, the specialised kernels of every sweep of a segment for an n-qubit
+ * state (host work only; no device is touched). Returns how many of the segment's structures have a
+ * ready kernel, or a negative error code for a malformed segment. */
+QSV_API int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n);
+
+/* Block until every queued background compilation has finished. */
+QSV_API int qsv_jit_wait(void);
+
+/* Counters of the specialised-kernel cache, written to out[0 .. min(cap, 8)): mode, structures seen,
+ * kernels ready, compilations failed, sweeps launched specialised, sweeps launched interpreted, total
+ * compile milliseconds, compilations queued or running. Returns 8. */
+QSV_API int qsv_jit_info(long long *out, int cap);
+
 #ifdef __cplusplus
 }
 #endif

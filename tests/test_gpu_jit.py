@@ -1,0 +1,120 @@
+"""GPU parity of the specialised sweep kernels (compiled at run time for each sweep structure), called
+through the C ABI. Bar: EXACT value equality with the C oracle and with the interpreter kernel, for every
+window size, both 13-qubit layouts and every op variant; the automatic mode switches to specialised
+kernels without changing a value."""
+import numpy as np
+import pytest
+
+import qsv_b200 as q
+from qsv_b200 import engine, generators as gen
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    (10, 8, lambda: gen.random_layer(10, 6, 11)),
+    (11, 9, lambda: gen.random_layer_ccx(11, 5, 12)),
+    (12, 12, lambda: gen.zoo(12, 3)),
+    (13, 10, lambda: gen.qft(13)),
+    (14, 12, lambda: gen.random_layer(14, 8, 13)),
+    (16, 12, lambda: gen.random_layer_ccx(16, 6, 14)),
+    (17, 7, lambda: gen.zoo(17, 4)),
+    (18, 12, lambda: gen.qft(18)),
+    (20, 12, lambda: gen.random_layer(20, 10, 0)),
+    (22, 12, lambda: gen.random_layer_ccx(22, 4, 15)),
+]
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    engine.load()
+    return t
+
+
+@pytest.fixture
+def jit_mode():
+    old = engine.set_jit("auto")
+    yield engine.set_jit
+    engine.set_jit(old)
+
+
+def _rand_state(n, seed):
+    rng = np.random.default_rng(seed)
+    x = (rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)).astype(np.complex64)
+    return (x / np.float32(np.linalg.norm(x))).astype(np.complex64)
+
+
+def _run(torch, x, seg):
+    t = torch.from_numpy(x.copy()).cuda()
+    engine.run_segment(t, seg)
+    torch.cuda.synchronize()
+    assert engine.device_status() == 0
+    return t.cpu().numpy()
+
+
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("rb", [4, 3])
+@pytest.mark.parametrize("n,k,maker", CASES)
+def test_specialised_exact_vs_oracle(torch, jit_mode, rb, n, k, maker):
+    jit_mode("eager")
+    engine.set_layout13(rb)
+    try:
+        prog, _, _ = q.compile_circuit(maker(), n, k)
+        x = _rand_state(n, n + rb)
+        before = engine.jit_info()["jit_launches"]
+        nsw = 0
+        for kind, seg in prog:
+            if kind == "segment":
+                nsw += len(engine.plan_segment(seg, n))
+                y = _run(torch, x, seg)
+                ref = orc.run_segment(x.copy(), seg)
+                assert np.array_equal(y, ref), f"n={n} rb={rb} max diff {np.max(np.abs(y - ref))}"
+                x = y
+            else:
+                x = orc.remap(x, seg)
+        info = engine.jit_info()
+        assert info["failed"] == 0 and info["jit_launches"] - before == nsw
+    finally:
+        engine.set_layout13(4)
+
+
+@pytest.mark.timeout(900)
+def test_specialised_equals_interpreter_large(torch, jit_mode):
+    """26 qubits (2^13 tiles per sweep, tensor-map and bulk staging): specialised == interpreter."""
+    n = 26
+    prog, _, _ = q.compile_circuit(gen.random_layer_ccx(n, 6, 5), n, 12)
+    segs = [s for kind, s in prog if kind == "segment"]
+    outs = []
+    for mode in ("off", "eager"):
+        jit_mode(mode)
+        t = engine.new_state(n)
+        for s in segs:
+            engine.run_segment(t, s)
+        torch.cuda.synchronize()
+        outs.append(t)
+    assert engine.device_status() == 0
+    assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.timeout(900)
+def test_auto_mode_switches_without_changing_values(torch, jit_mode):
+    n = 20
+    jit_mode("auto")
+    prog, _, _ = q.compile_circuit(gen.random_layer(n, 12, 77), n, 12)
+    segs = [s for kind, s in prog if kind == "segment"]
+    x = _rand_state(n, 5)
+    ref = x.copy()
+    for s in segs:
+        orc.run_segment(ref, s)
+    for it in range(4):
+        t = torch.from_numpy(x.copy()).cuda()
+        for s in segs:
+            engine.run_segment(t, s)
+        torch.cuda.synchronize()
+        assert np.array_equal(t.cpu().numpy(), ref), it
+        engine.jit_wait()
+    info = engine.jit_info()
+    assert info["failed"] == 0 and info["jit_launches"] > 0

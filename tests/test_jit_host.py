@@ -1,0 +1,70 @@
+"""Specialised sweep kernels, host side: the generated CUDA source compiles (NVRTC, sm_100a) for every sweep
+structure of a varied set of circuits -- all window sizes 10..13, both 13-qubit layouts, every op variant
+and slot -- with no device involved. Their values are checked against the oracle in test_gpu_jit.py."""
+import collections
+
+import pytest
+
+import qsv_b200 as q
+from qsv_b200 import engine, generators as gen
+
+CIRCUITS = [
+    (10, 8, lambda: gen.random_layer(10, 4, 1)),
+    (11, 9, lambda: gen.random_layer_ccx(11, 3, 2)),
+    (12, 12, lambda: gen.zoo(12, 3)),
+    (16, 12, lambda: gen.zoo(16, 5)),
+    (17, 7, lambda: gen.random_layer_ccx(17, 3, 4)),
+    (18, 12, lambda: gen.qft(18)),
+]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return engine.load()
+
+
+def _variants(prog, n):
+    seen = collections.Counter()
+    for kind, seg in prog:
+        if kind == "segment":
+            for sw in engine.plan_segment(seg, n):
+                for o in sw["ops"]:
+                    slot = "comp" if o["slot"] == 0 else ("reg" if o["slot"] < 8 else "lane")
+                    seen[(slot, o["variant"])] += 1
+    return seen
+
+
+@pytest.mark.timeout(900)
+def test_specialised_kernels_compile(lib):
+    variants = collections.Counter()
+    for rb in (4, 3):
+        engine.set_layout13(rb)
+        try:
+            for n, k, make in CIRCUITS:
+                prog, _, _ = q.compile_circuit(make(), n, k)
+                variants.update(_variants(prog, n))
+                for kind, seg in prog:
+                    if kind == "segment":
+                        nsw = len(engine.plan_segment(seg, n))
+                        assert engine.jit_prepare(seg, n) == nsw, lib.qsv_last_error().decode()
+        finally:
+            engine.set_layout13(4)
+    info = engine.jit_info()
+    assert info["failed"] == 0 and info["ready"] == info["structures"] > 10 and info["pending"] == 0
+    # every slot kind and the common variants were generated
+    slots = {s for s, _ in variants}
+    assert slots == {"comp", "reg", "lane"}
+    vs = {v for _, v in variants}
+    assert {1, 2, 3, 4, 5, 6, 7}.issubset(vs), sorted(vs)
+
+
+def test_jit_mode_switch(lib):
+    old = engine.set_jit("off")
+    try:
+        assert engine.jit_info()["mode"] == 0
+        assert engine.set_jit("eager") == "off"
+        assert engine.jit_info()["mode"] == 1
+        with pytest.raises(engine.QSVError):
+            engine.set_jit(7)
+    finally:
+        engine.set_jit(old)

@@ -29,6 +29,12 @@ cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
 cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
 cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
+int jit_set_mode(int mode);
+int jit_prepare(const std::vector<QsvSweep> &sweeps);
+void jit_wait();
+int jit_info(long long *out, int cap);
+std::string jit_last_log();
+int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream, cudaError_t *err);
 }  // namespace qsv
 
 static thread_local std::string t_err;
@@ -110,11 +116,48 @@ int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int d
     const int nsm = sm_count();
     std::lock_guard<std::mutex> lk(g_launch_mu);
     for (const QsvSweep &sw : sweeps) {
-        cudaError_t e = qsv::launch_sweep((float2 *)state, sw, nsm, (cudaStream_t)stream);
-        if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+        cudaError_t e = cudaSuccess;
+        const int r = qsv::jit_try_launch((float2 *)state, sw, nsm, (cudaStream_t)stream, &e);
+        if (r < 0) return cuda_fail(e, "specialised sweep launch");
+        if (r == 0) {
+            e = qsv::launch_sweep((float2 *)state, sw, nsm, (cudaStream_t)stream);
+            if (e != cudaSuccess) return cuda_fail(e, "sweep launch");
+        }
         t_launches++;
     }
     return QSV_OK;
+}
+
+int qsv_set_jit(int mode) {
+    const int old = qsv::jit_set_mode(mode);
+    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "jit mode must be 0, 1 or 2");
+    return old;
+}
+
+int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n) {
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    std::vector<qsv::PhysPass> passes;
+    std::string err;
+    int rc = qsv::decode_segment(seg, nwords, n, passes, err);
+    if (rc) return fail(rc, err);
+    std::vector<QsvSweep> sweeps;
+    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    if (rc) return fail(rc, err);
+    const int ready = qsv::jit_prepare(sweeps);
+    const std::string log = qsv::jit_last_log();
+    if (!log.empty()) t_err = log;
+    return ready;
+}
+
+int qsv_jit_wait(void) {
+    qsv::jit_wait();
+    return QSV_OK;
+}
+
+int qsv_jit_info(long long *out, int cap) {
+    if (!out || cap < 0) return fail(QSV_ERR_INVALID_ARG, "null output");
+    return qsv::jit_info(out, cap);
 }
 
 int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, void *stream) {

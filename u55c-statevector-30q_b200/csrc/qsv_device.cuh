@@ -1,10 +1,16 @@
 // qsv_device.cuh -- sm_100a device helpers: mbarriers, bulk-async (TMA engine) copies, proxy fences,
 // bounded waits, and the MUX2 pair arithmetic.
 #pragma once
-#include <cuda_runtime.h>
-#include <stdint.h>
-
 #include "qsv_plan.h"
+#ifdef __CUDACC_RTC__
+// the tensor-map parameter of a sweep kernel: 128 opaque bytes, 64-byte aligned (cuda.h's CUtensorMap)
+struct alignas(64) CUtensorMap {
+    unsigned long long opaque[16];
+};
+#else
+#include <cuda.h>
+#include <cuda_runtime.h>
+#endif
 
 namespace qsv {
 namespace dev {

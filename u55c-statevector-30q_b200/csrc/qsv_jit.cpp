@@ -1,0 +1,379 @@
+// qsv_jit.cpp -- sweep kernels specialised to one sweep structure, generated and compiled at run time.
+//
+// No reference counterpart (the reference's engine is one fixed HLS kernel). The interpreter kernel
+// (qsv_sweep.cu) reads every op's slot, variant and controls at run time; a specialised kernel has them as
+// template arguments (qsv_jit_ops.cuh), so per-op dispatch, control tests on register bits and layout
+// arithmetic vanish from the inner loop. A sweep's *structure* is everything but its matrices, window and
+// tile addressing: window size, phase layouts, and per op the target slot, code variant and control masks.
+// Circuits repeat structures (a 30-qubit random-layer circuit of depth 24 has 84 sweeps of 7 structures),
+// so each structure is compiled once per process with NVRTC (sm_100a cubin from the engine's own device
+// headers, embedded at build time) and loaded into every device that runs it. Matrices, window and tile
+// addressing stay kernel parameters. Specialised and interpreted sweeps compute the same values.
+//
+// Modes: 0 = interpreter only; 1 = eager (a new structure is compiled before its first launch);
+// 2 = automatic (default): a structure is compiled in the background once it has been launched
+// kThreshold times, and launches use the interpreter until its kernel is ready.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "qsv_planner.h"
+#include "_gen/qsv_jit_headers.inc"
+
+namespace qsv {
+namespace dev {
+cudaError_t make_tmap(CUtensorMap *map, float2 *state, const QsvSweep &sw);
+}
+cudaError_t status_word_ptr(int **out);
+
+namespace {
+
+constexpr int kThreshold = 2;      // launches of a structure before automatic mode compiles it
+constexpr int kMaxDevices = 64;
+constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
+
+struct Drv {
+    PFN_cuModuleLoadData_v2000 module_load = nullptr;
+    PFN_cuModuleGetFunction_v2000 get_function = nullptr;
+    PFN_cuFuncSetAttribute_v9000 set_attribute = nullptr;
+    PFN_cuLaunchKernel_v4000 launch = nullptr;
+    PFN_cuOccupancyMaxActiveBlocksPerMultiprocessor_v6050 occupancy = nullptr;
+    bool ok = false;
+};
+
+const Drv &drv() {
+    static const Drv d = [] {
+        Drv x;
+        auto get = [](const char *name, void **p) {
+            cudaDriverEntryPointQueryResult q;
+            return cudaGetDriverEntryPoint(name, p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess;
+        };
+        x.ok = get("cuModuleLoadData", reinterpret_cast<void **>(&x.module_load)) &&
+               get("cuModuleGetFunction", reinterpret_cast<void **>(&x.get_function)) &&
+               get("cuFuncSetAttribute", reinterpret_cast<void **>(&x.set_attribute)) &&
+               get("cuLaunchKernel", reinterpret_cast<void **>(&x.launch)) &&
+               get("cuOccupancyMaxActiveBlocksPerMultiprocessor", reinterpret_cast<void **>(&x.occupancy));
+        return x;
+    }();
+    return d;
+}
+
+enum State { kNew, kQueued, kReady, kFailed };
+
+struct Entry {
+    int kw = 0, rb = 0, wb = 0;
+    std::string src;
+    State state = kNew;
+    std::vector<char> cubin;
+    std::string log;
+    long long uses = 0;
+    CUfunction fn[kMaxDevices] = {nullptr};
+    int per_sm[kMaxDevices] = {0};
+};
+
+struct Jit {
+    std::mutex mu;
+    std::condition_variable work, done;
+    std::unordered_map<std::string, std::shared_ptr<Entry>> map;
+    std::deque<std::shared_ptr<Entry>> queue;
+    int threads = 0, busy = 0;
+    int mode = 2;
+    long long jit_launches = 0, interp_launches = 0, compiled = 0, failed = 0;
+    double compile_ms = 0.0;
+    std::string last_log;
+};
+
+// process-lifetime state (never destroyed: detached compile threads may still wait on it at exit)
+Jit &J() {
+    static Jit *j = new Jit;
+    return *j;
+}
+
+std::string key_of(const QsvSweep &sw, int rb, int wb) {
+    std::string k;
+    auto put = [&](int v) { k.push_back((char)(v & 0xff)); };
+    auto put32 = [&](uint32_t v) { k.append(reinterpret_cast<const char *>(&v), 4); };
+    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops);
+    for (int p = 0; p < sw.nphases; p++) {
+        const QsvPhase &ph = sw.phases[p];
+        for (int r = 0; r < rb; r++) put(ph.reg_bits[r]);
+        put(ph.lane_bits[0]); put(ph.lane_bits[1]);
+        for (int w = 0; w < wb; w++) put(ph.warp_bits[w]);
+        put(ph.op_begin); put(ph.op_end);
+    }
+    for (int o = 0; o < sw.nops; o++) {
+        const QsvOp &op = sw.ops[o];
+        put(op.slot); put(op.variant); put(op.cm_reg); put32(op.cm_thr);
+    }
+    return k;
+}
+
+// CUDA source of the kernel specialised to sw's structure
+std::string gen_source(const QsvSweep &sw, int rb, int wb) {
+    const int nc = 1 << (5 + wb), nt = nc + 32, minb = sw.kw >= 13 ? 1 : 2;
+    std::ostringstream s;
+    s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
+      << "namespace qsv {\nnamespace dev {\nstruct JitBody {\n"
+      << "    static constexpr bool kSmemOps = false;\n"
+      << "    template <int NV, int RB, int WB>\n"
+      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *, int lane, int warp) {\n";
+    for (int p = 0; p < sw.nphases; p++) {
+        const QsvPhase &ph = sw.phases[p];
+        if (p > 0) s << "        named_bar_sync(1, " << nc << ");\n";
+        s << "        {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_bits[0] << ", "
+          << (int)ph.lane_bits[1] << ">(lane)";
+        for (int w = 0; w < wb; w++) s << " | jit_warp_bit<" << (int)ph.warp_bits[w] << ">(warp, " << w << ")";
+        s << ";\n            float2 R[NV], I[NV];\n";
+        std::string rbits;
+        for (int r = 0; r < rb; r++) rbits += (r ? ", " : "") + std::to_string((int)ph.reg_bits[r]);
+        s << "            jit_load<NV, " << rbits << ">(tile, tb, R, I);\n";
+        for (int o = ph.op_begin; o < ph.op_end; o++) {
+            const QsvOp &op = sw.ops[o];
+            const std::string thr = std::to_string(op.cm_thr) + "u";
+            if (op.slot == QSV_SLOT_COMP)
+                s << "            jit_comp<NV, " << thr << ">(R, I, P.ops[" << o << "], tb);\n";
+            else if (op.slot < QSV_SLOT_LANE0)
+                s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << (int)op.variant << ", "
+                  << (int)op.cm_reg << ", " << thr << ">(R, I, P.ops[" << o << "], tb);\n";
+            else
+                s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", "
+                  << (int)op.cm_reg << ", " << thr << ">(R, I, P.ops[" << o << "], tb, lane);\n";
+        }
+        s << "            jit_store<NV, " << rbits << ">(tile, tb, R, I);\n        }\n";
+    }
+    s << "    }\n};\n}  // namespace dev\n}  // namespace qsv\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb << ")\n"
+      << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
+      << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
+      << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages
+      << ", qsv::dev::JitBody>(state, P, &tmap, status);\n}\n";
+    return s.str();
+}
+
+bool nvrtc_compile(const std::string &src, std::vector<char> &cubin, std::string &log) {
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src.c_str(), "qsv_sweep_jit.cu", kJitNumHeaders, kJitHeaderSources,
+                           kJitHeaderNames) != NVRTC_SUCCESS) {
+        log = "nvrtcCreateProgram failed";
+        return false;
+    }
+    // QSV_JIT_PTXAS_VERBOSE=1 keeps ptxas's resource report (registers, spills) in the compile log
+    const bool verbose = std::getenv("QSV_JIT_PTXAS_VERBOSE") != nullptr;
+    const char *opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-DQSV_JIT=1", "--ptxas-options=-v"};
+    const nvrtcResult r = nvrtcCompileProgram(prog, verbose ? 4 : 3, opts);
+    size_t ls = 0;
+    nvrtcGetProgramLogSize(prog, &ls);
+    log.assign(ls, '\0');
+    if (ls) nvrtcGetProgramLog(prog, &log[0]);
+    bool ok = r == NVRTC_SUCCESS;
+    if (ok) {
+        size_t n = 0;
+        ok = nvrtcGetCUBINSize(prog, &n) == NVRTC_SUCCESS && n > 0;
+        if (ok) {
+            cubin.resize(n);
+            ok = nvrtcGetCUBIN(prog, cubin.data()) == NVRTC_SUCCESS;
+        }
+    } else {
+        log = std::string(nvrtcGetErrorString(r)) + ": " + log;
+    }
+    nvrtcDestroyProgram(&prog);
+    return ok;
+}
+
+void worker() {
+    Jit &j = J();
+    std::unique_lock<std::mutex> lk(j.mu);
+    for (;;) {
+        j.work.wait(lk, [&] { return !j.queue.empty(); });
+        std::shared_ptr<Entry> e = j.queue.front();
+        j.queue.pop_front();
+        j.busy++;
+        const std::string src = e->src;
+        lk.unlock();
+        std::vector<char> cubin;
+        std::string log;
+        const auto t0 = std::chrono::steady_clock::now();
+        const bool ok = nvrtc_compile(src, cubin, log);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        lk.lock();
+        e->cubin = std::move(cubin);
+        e->log = log;
+        e->state = ok ? kReady : kFailed;
+        if (ok) j.compiled++;
+        else j.failed++;
+        if (!ok || std::getenv("QSV_JIT_PTXAS_VERBOSE")) j.last_log = log;
+        j.compile_ms += ms;
+        j.busy--;
+        j.done.notify_all();
+    }
+}
+
+// with j.mu held: queue e for compilation (starts the compile threads on first use)
+void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
+    if (e->state != kNew) return;
+    e->src = gen_source(sw, e->rb, e->wb);
+    e->state = kQueued;
+    j.queue.push_back(e);
+    if (j.threads == 0) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int n = std::max(1, std::min(8, (int)(hw ? hw / 2 : 2)));
+        for (int i = 0; i < n; i++) std::thread(worker).detach();
+        j.threads = n;
+    }
+    j.work.notify_one();
+}
+
+std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
+    const std::string key = key_of(sw, rb, wb);
+    auto it = j.map.find(key);
+    if (it != j.map.end()) return it->second;
+    auto e = std::make_shared<Entry>();
+    e->kw = sw.kw;
+    e->rb = rb;
+    e->wb = wb;
+    j.map.emplace(key, e);
+    return e;
+}
+
+}  // namespace
+
+int jit_set_mode(int mode) {
+    if (mode < 0 || mode > 2) return -1;
+    Jit &j = J();
+    std::lock_guard<std::mutex> lk(j.mu);
+    const int old = j.mode;
+    j.mode = mode;
+    return old;
+}
+
+// Compile (in parallel, blocking) every structure of the given sweeps that is not compiled yet.
+// Returns the number of those structures whose kernel is ready.
+int jit_prepare(const std::vector<QsvSweep> &sweeps) {
+    Jit &j = J();
+    std::unique_lock<std::mutex> lk(j.mu);
+    std::vector<std::shared_ptr<Entry>> mine;
+    for (const QsvSweep &sw : sweeps) {
+        int rb = 0, wb = 0;
+        if (layout_for_kw(sw.kw, &rb, &wb)) continue;
+        auto e = find_or_add(j, sw, rb, wb);
+        enqueue(j, e, sw);
+        mine.push_back(e);
+    }
+    j.done.wait(lk, [&] {
+        for (auto &e : mine)
+            if (e->state == kQueued) return false;
+        return true;
+    });
+    int ready = 0;
+    for (auto &e : mine) ready += e->state == kReady;
+    return ready;
+}
+
+void jit_wait() {
+    Jit &j = J();
+    std::unique_lock<std::mutex> lk(j.mu);
+    j.done.wait(lk, [&] { return j.queue.empty() && j.busy == 0; });
+}
+
+// stats: mode, structures, ready, failed, launches specialised, launches interpreted, compile ms, queued
+int jit_info(long long *out, int cap) {
+    Jit &j = J();
+    std::lock_guard<std::mutex> lk(j.mu);
+    long long ready = 0;
+    for (auto &kv : j.map) ready += kv.second->state == kReady;
+    const long long v[8] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
+                            (long long)j.compile_ms, (long long)(j.queue.size() + j.busy)};
+    const int n = std::min(cap, 8);
+    for (int i = 0; i < n; i++) out[i] = v[i];
+    return 8;
+}
+
+std::string jit_last_log() {
+    Jit &j = J();
+    std::lock_guard<std::mutex> lk(j.mu);
+    return j.last_log;
+}
+
+// Launch sw with its specialised kernel if that kernel is ready (compiling it first in eager mode).
+// Returns 1 if launched, 0 if the caller should run the interpreter, -1 on a CUDA error (*err set).
+int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream, cudaError_t *err) {
+    Jit &j = J();
+    int rb = 0, wb = 0;
+    if (layout_for_kw(sw.kw, &rb, &wb)) return 0;
+    const Drv &d = drv();
+    std::shared_ptr<Entry> e;
+    {
+        std::unique_lock<std::mutex> lk(j.mu);
+        if (j.mode == 0 || !d.ok) { j.interp_launches++; return 0; }
+        e = find_or_add(j, sw, rb, wb);
+        e->uses++;
+        if (e->state == kNew && (j.mode == 1 || e->uses >= kThreshold)) enqueue(j, e, sw);
+        if (j.mode == 1) j.done.wait(lk, [&] { return e->state != kQueued; });
+        if (e->state != kReady) { j.interp_launches++; return 0; }
+    }
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
+    const int NT = (1 << (5 + wb)) + 32;
+    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2);
+    if (!e->fn[dev]) {
+        // loading a module is not a stream operation: keep it out of stream captures
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            std::lock_guard<std::mutex> lk(j.mu);
+            j.interp_launches++;
+            return 0;
+        }
+        ce = cudaSetDevice(dev);      // makes the device's primary context current on this thread
+        if (ce != cudaSuccess) { *err = ce; return -1; }
+        CUmodule mod = nullptr;
+        CUfunction fn = nullptr;
+        int per_sm = 0;
+        if (d.module_load(&mod, e->cubin.data()) != CUDA_SUCCESS ||
+            d.get_function(&fn, mod, "qsv_sweep_jit") != CUDA_SUCCESS ||
+            d.set_attribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem) != CUDA_SUCCESS ||
+            d.occupancy(&per_sm, fn, NT, smem) != CUDA_SUCCESS) {
+            *err = cudaErrorInvalidKernelImage;
+            return -1;
+        }
+        std::lock_guard<std::mutex> lk(j.mu);
+        e->per_sm[dev] = per_sm < 1 ? 1 : per_sm;
+        e->fn[dev] = fn;
+    }
+    alignas(64) CUtensorMap map;
+    ce = dev::make_tmap(&map, state, sw);
+    if (ce != cudaSuccess) { *err = ce; return -1; }
+    int *status = nullptr;
+    ce = status_word_ptr(&status);
+    if (ce != cudaSuccess) { *err = ce; return -1; }
+    int64_t grid = (int64_t)nsm * e->per_sm[dev];
+    if (grid > sw.ntiles) grid = sw.ntiles;
+    void *args[] = {&state, const_cast<QsvSweep *>(&sw), &map, &status};
+    if (d.launch(e->fn[dev], (unsigned)grid, 1, 1, (unsigned)NT, 1, 1, (unsigned)smem, (CUstream)stream, args,
+                 nullptr) != CUDA_SUCCESS) {
+        *err = cudaErrorLaunchFailure;
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(j.mu);
+    j.jit_launches++;
+    return 1;
+}
+
+}  // namespace qsv

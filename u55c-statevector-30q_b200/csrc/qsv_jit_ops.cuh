@@ -1,0 +1,239 @@
+// qsv_jit_ops.cuh -- MUX2 op application with the op's structure fixed at compile time.
+//
+// Used by sweep kernels specialised to one sweep structure (generated and compiled at run time by
+// qsv_jit.cpp). Target slot, code variant, register-control mask and thread-control mask are template
+// arguments, so per-op dispatch disappears, controls on register bits resolve at compile time (a
+// controlled swap on register bits becomes a register renaming), and the phase layout's shared-memory
+// offsets become immediates. The matrices stay data: they are read from the kernel's parameter block at
+// fixed offsets. Every update uses the interpreter's arithmetic (qsv_ops.cuh / qsv_device.cuh); forms
+// that skip work only skip exact-zero terms or unselected pairs, so values equal the interpreter's and the
+// CPU oracle's (up to the sign of a zero).
+#pragma once
+#include "qsv_ops.cuh"
+
+namespace qsv {
+namespace dev {
+
+// thread base of a phase: tile bits 1-3 from lane bits 0-2, lane bits 3-4 on tile bits LB0 / LB1
+template <int LB0, int LB1>
+__device__ __forceinline__ uint32_t jit_lane_base(int lane) {
+    return ((uint32_t)(lane & 7) << 1) | ((uint32_t)((lane >> 3) & 1) << LB0) | ((uint32_t)((lane >> 4) & 1) << LB1);
+}
+template <int WBIT>
+__device__ __forceinline__ uint32_t jit_warp_bit(int warp, int w) {
+    return (uint32_t)((warp >> w) & 1) << WBIT;
+}
+
+// offset of register slot r in a phase whose register bits are the tile bits RBITS...
+template <int... RBITS>
+__device__ __forceinline__ constexpr uint32_t jit_reg_off(int r) {
+    constexpr int bits[] = {RBITS...};
+    uint32_t o = 0;
+    for (int q = 0; q < (int)sizeof...(RBITS); q++)
+        if ((r >> q) & 1) o += 1u << bits[q];
+    return o;
+}
+
+template <int NV, int... RBITS>
+__device__ __forceinline__ void jit_load(const float2 *tile, uint32_t tb, float2 (&R)[NV], float2 (&I)[NV]) {
+#pragma unroll
+    for (int r = 0; r < NV; r++) {
+        const float4 v = *reinterpret_cast<const float4 *>(tile + tb + jit_reg_off<RBITS...>(r));
+        R[r] = make_float2(v.x, v.z);
+        I[r] = make_float2(v.y, v.w);
+    }
+}
+template <int NV, int... RBITS>
+__device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float2 (&R)[NV], const float2 (&I)[NV]) {
+#pragma unroll
+    for (int r = 0; r < NV; r++)
+        *reinterpret_cast<float4 *>(tile + tb + jit_reg_off<RBITS...>(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+}
+
+__device__ __forceinline__ void jit_mat(float (&m)[8], const float *src) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) m[e] = src[e];
+}
+
+// ---------------------------------------------------------------- register-bit target
+template <int NV, int RBIT, int VAR, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ void jit_reg(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
+    constexpr int B = 1 << RBIT;
+    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
+    if constexpr (VAR == QSV_V_SKIP) {
+        return;
+    } else if constexpr (VAR == QSV_V_UNI_DENSE) {
+        float m[8];
+        jit_mat(m, op.m0);
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            if (!(r & B)) dense2(R[r], I[r], R[r | B], I[r | B], m);
+    } else if constexpr (VAR == QSV_V_UNI_DIAG) {
+        const float a0 = op.m0[0], a1 = op.m0[1], d0 = op.m0[6], d1 = op.m0[7];
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            if (!(r & B)) { cmul2(R[r], I[r], a0, a1); cmul2(R[r | B], I[r | B], d0, d1); }
+    } else if constexpr (VAR == QSV_V_UNI_SWAP) {
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            if (!(r & B)) { swap2(R[r], R[r | B]); swap2(I[r], I[r | B]); }
+    } else if constexpr (VAR == QSV_V_CTRL_DENSE) {
+        float m[8];
+        jit_mat(m, op.m1);
+        if (tok) {
+#pragma unroll
+            for (int r = 0; r < NV; r++)
+                if (!(r & B) && (r & CMREG) == CMREG) dense2(R[r], I[r], R[r | B], I[r | B], m);
+        }
+    } else if constexpr (VAR == QSV_V_CTRL_DIAG1) {
+        const float d0 = op.m1[6], d1 = op.m1[7];
+        if (tok) {
+#pragma unroll
+            for (int r = 0; r < NV; r++)
+                if (!(r & B) && (r & CMREG) == CMREG) cmul2(R[r | B], I[r | B], d0, d1);
+        }
+    } else if constexpr (VAR == QSV_V_CTRL_SWAP) {
+        if (CMTHR == 0u) {
+#pragma unroll
+            for (int r = 0; r < NV; r++)
+                if (!(r & B) && (r & CMREG) == CMREG) { swap2(R[r], R[r | B]); swap2(I[r], I[r | B]); }
+        } else if (tok) {
+#pragma unroll
+            for (int r = 0; r < NV; r++)
+                if (!(r & B) && (r & CMREG) == CMREG) { swap2(R[r], R[r | B]); swap2(I[r], I[r | B]); }
+        }
+    } else if constexpr (VAR == QSV_V_CTRL_DENSE_SEL) {
+        const float id[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f};
+        float m[8];
+        jit_mat(m, op.m1);
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & B) || (r & CMREG) != CMREG) continue;
+            float c[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) c[e] = tok ? m[e] : id[e];
+            dense2(R[r], I[r], R[r | B], I[r | B], c);
+        }
+    } else if constexpr (VAR == QSV_V_CTRL_DIAG1_SEL) {
+        const float d0 = tok ? op.m1[6] : 1.f, d1 = tok ? op.m1[7] : 0.f;
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            if (!(r & B) && (r & CMREG) == CMREG) cmul2(R[r | B], I[r | B], d0, d1);
+    } else if constexpr (VAR == QSV_V_CTRL_SWAP_SEL) {
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & B) || (r & CMREG) != CMREG) continue;
+            const float2 a = R[r], b = R[r | B], c = I[r], d = I[r | B];
+            R[r] = tok ? b : a; R[r | B] = tok ? a : b;
+            I[r] = tok ? d : c; I[r | B] = tok ? c : d;
+        }
+    } else {
+        float m0[8], m1[8];
+        jit_mat(m0, op.m0);
+        jit_mat(m1, op.m1);
+        reg_op<NV, RBIT>(R, I, op, m0, m1, tok);
+    }
+}
+
+// ---------------------------------------------------------------- lane-bit target (LB = lane bit 0..4)
+// For an output amplitude "own" with partner "oth" on lane ^ (1 << LB): y = a*own + b*oth, (a, b) =
+// (m00, m01) on the bit-0 side and (m11, m10) on the bit-1 side -- the interpreter's lane update.
+__device__ __forceinline__ void jit_lane_lin(float2 &R, float2 &I, const float2 oR, const float2 oI, const float2 ar,
+                                             const float2 ai, const float2 nai, const float2 br, const float2 bi,
+                                             const float2 nbi) {
+    float2 t = __fmul2_rn(nbi, oI);
+    t = __ffma2_rn(br, oR, t);
+    t = __ffma2_rn(nai, I, t);
+    const float2 yr = __ffma2_rn(ar, R, t);
+    float2 u = __fmul2_rn(bi, oR);
+    u = __ffma2_rn(br, oI, u);
+    u = __ffma2_rn(ai, R, u);
+    const float2 yi = __ffma2_rn(ar, I, u);
+    R = yr;
+    I = yi;
+}
+__device__ __forceinline__ void jit_shfl(const float2 &R, const float2 &I, float2 &oR, float2 &oI, int xm) {
+    oR.x = __shfl_xor_sync(0xffffffffu, R.x, xm);
+    oR.y = __shfl_xor_sync(0xffffffffu, R.y, xm);
+    oI.x = __shfl_xor_sync(0xffffffffu, I.x, xm);
+    oI.y = __shfl_xor_sync(0xffffffffu, I.y, xm);
+}
+
+template <int NV, int LB, int VAR, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb, int lane) {
+    constexpr int XM = 1 << LB;
+    const bool mine = (lane >> LB) & 1;
+    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
+    if constexpr (VAR == QSV_V_SKIP) {
+        return;
+    } else if constexpr (VAR == QSV_V_UNI_DENSE || VAR == QSV_V_CTRL_DENSE || VAR == QSV_V_CTRL_DENSE_SEL) {
+        constexpr bool UNI = VAR == QSV_V_UNI_DENSE;
+        const float *m = UNI ? op.m0 : op.m1;
+        const float a_r = mine ? m[6] : m[0], a_i = mine ? m[7] : m[1];
+        const float b_r = mine ? m[4] : m[2], b_i = mine ? m[5] : m[3];
+        const float2 ar = f2(a_r), ai = f2(a_i), nai = f2(-a_i), br = f2(b_r), bi = f2(b_i), nbi = f2(-b_i);
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if (!UNI && (r & CMREG) != CMREG) continue;
+            float2 oR, oI;
+            jit_shfl(R[r], I[r], oR, oI, XM);
+            float2 yR = R[r], yI = I[r];
+            jit_lane_lin(yR, yI, oR, oI, ar, ai, nai, br, bi, nbi);
+            if (UNI || CMTHR == 0u) {
+                R[r] = yR; I[r] = yI;
+            } else {
+                R[r] = tok ? yR : R[r];
+                I[r] = tok ? yI : I[r];
+            }
+        }
+    } else if constexpr (VAR == QSV_V_UNI_DIAG) {
+        // diagonal: each amplitude is scaled by its own diagonal entry, no exchange
+        const float a_r = mine ? op.m0[6] : op.m0[0], a_i = mine ? op.m0[7] : op.m0[1];
+#pragma unroll
+        for (int r = 0; r < NV; r++) cmul2(R[r], I[r], a_r, a_i);
+    } else if constexpr (VAR == QSV_V_CTRL_DIAG1 || VAR == QSV_V_CTRL_DIAG1_SEL) {
+        // diag(1, d) where selected: only the bit-1 side changes
+        const bool s = mine && tok;
+        const float d_r = op.m1[6], d_i = op.m1[7];
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & CMREG) != CMREG) continue;
+            float2 yR = R[r], yI = I[r];
+            cmul2(yR, yI, d_r, d_i);
+            R[r] = s ? yR : R[r];
+            I[r] = s ? yI : I[r];
+        }
+    } else if constexpr (VAR == QSV_V_UNI_SWAP || VAR == QSV_V_CTRL_SWAP || VAR == QSV_V_CTRL_SWAP_SEL) {
+        constexpr bool UNI = VAR == QSV_V_UNI_SWAP;
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if (!UNI && (r & CMREG) != CMREG) continue;
+            float2 oR, oI;
+            jit_shfl(R[r], I[r], oR, oI, XM);
+            if (UNI || CMTHR == 0u) {
+                R[r] = oR; I[r] = oI;
+            } else {
+                R[r] = tok ? oR : R[r];
+                I[r] = tok ? oI : I[r];
+            }
+        }
+    } else {
+        float m0[8], m1[8];
+        jit_mat(m0, op.m0);
+        jit_mat(m1, op.m1);
+        lane_op<NV>(R, I, op, m0, m1, tok, LB, lane);
+    }
+}
+
+// ---------------------------------------------------------------- tile-bit-0 target (halves of a float4)
+template <int NV, uint32_t CMTHR>
+__device__ __forceinline__ void jit_comp(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
+    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
+    float m0[8], m1[8];
+    jit_mat(m0, op.m0);
+    jit_mat(m1, op.m1);
+    comp_op<NV>(R, I, op, m0, m1, tok);
+}
+
+}  // namespace dev
+}  // namespace qsv

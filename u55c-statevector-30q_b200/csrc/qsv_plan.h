@@ -25,7 +25,17 @@
 // An op can run in a phase when its target is tile bit 0..3, a register bit or a lane bit of that phase;
 // controls may sit anywhere in the window.
 #pragma once
+#ifdef __CUDACC_RTC__
+// compiled at run time by NVRTC (sweep kernels specialised to one structure): no host headers there
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#else
 #include <stdint.h>
+#endif
 
 #define QSV_KW_MAX 13
 #define QSV_RB_MAX 4

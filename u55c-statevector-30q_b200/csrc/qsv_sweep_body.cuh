@@ -1,0 +1,203 @@
+// qsv_sweep_body.cuh -- the sweep pipeline shared by every sweep kernel (sm_100a).
+//
+// Replaces the reader / writer stages of the reference's HLS engine (kernels/sv/sv_engine.cpp:86-152,
+// DATAFLOW per pass). One persistent CTA per SM, grid-strided over the 2^(n-KW) tiles of a sweep:
+//   * a producer warp streams tiles HBM -> shared memory and back with the TMA engine: one tensor-map box
+//     per tile when the window's contiguous runs are short, one bulk-async copy per sub-block when they
+//     are long; completion is counted on mbarriers, up to S tiles are in flight;
+//   * consumer warps run Body::tile on each staged tile (the ops of the sweep, in registers).
+// Body is the interpreter (qsv_sweep.cu: op table read at run time) or a kernel specialised to one sweep
+// structure (qsv_jit.cpp: ops fixed at compile time). Both run the same arithmetic (qsv_ops.cuh).
+// The tile addressing is the reference's (host/sv/model.py:25-40, sv_engine.cpp:61-84,116): tile T's
+// base is pdep(T, free bits) and sub-block s sits at base | pdep(s, H).
+#pragma once
+#include "qsv_device.cuh"
+
+namespace qsv {
+namespace dev {
+
+// ---------------------------------------------------------------- tensor-map TMA
+__device__ __forceinline__ void tma_load(void *sdst, const CUtensorMap *map, const int32_t *c, int rank, uint64_t *bar) {
+    const uint64_t m = reinterpret_cast<uint64_t>(map);
+    const uint32_t d = smem_u32(sdst), b = smem_u32(bar);
+    switch (rank) {
+        case 2:
+            asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                         ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(b) : "memory");
+            break;
+        case 3:
+            asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                         ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(b) : "memory");
+            break;
+        case 4:
+            asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                         ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(b) : "memory");
+            break;
+        default:
+            asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                         ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(b) : "memory");
+            break;
+    }
+}
+__device__ __forceinline__ void tma_store(const CUtensorMap *map, const int32_t *c, int rank, const void *ssrc) {
+    const uint64_t m = reinterpret_cast<uint64_t>(map);
+    const uint32_t s = smem_u32(ssrc);
+    switch (rank) {
+        case 2:
+            asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                         ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(s) : "memory");
+            break;
+        case 3:
+            asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];"
+                         ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(s) : "memory");
+            break;
+        case 4:
+            asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+                         ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(s) : "memory");
+            break;
+        default:
+            asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];"
+                         ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(s) : "memory");
+            break;
+    }
+}
+
+// Dynamic shared memory a sweep kernel needs: S tile buffers, plus the op table when Body reads it there.
+template <int KW, int S>
+__host__ __device__ constexpr size_t sweep_smem_bytes(bool smem_ops) {
+    return ((size_t)S << KW) * 8 + (smem_ops ? sizeof(QsvOp) * QSV_MAX_SWEEP_OPS : 0);
+}
+
+// The pipeline. Launch with (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S>(Body::kSmemOps) bytes
+// of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
+template <int KW, int RB, int WB, int S, class Body>
+__device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const QsvSweep &P, const CUtensorMap *tmap,
+                                               int *status) {
+    constexpr int NC = 1 << (5 + WB);        // consumer threads
+    constexpr int NV = 1 << RB;              // float4 per consumer thread
+    constexpr int TILE = 1 << KW;            // amplitudes per tile
+    static_assert(1 + 3 + 2 + RB + WB == KW, "layout must cover the window");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    float2 *bufs = reinterpret_cast<float2 *>(smem_raw);
+    // the interpreter's op table, copied once from the parameter block: shared-memory reads of an op's
+    // fields are independent short-latency loads (the constant-bank path serialises run-time indices)
+    QsvOp *sops = reinterpret_cast<QsvOp *>(smem_raw + ((size_t)S << KW) * sizeof(float2));
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t done[S];
+    __shared__ volatile int abort_flag;
+
+    const int tid = threadIdx.x;
+    if (Body::kSmemOps) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(P.ops);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(sops);
+        const int words = P.nops * (int)(sizeof(QsvOp) / 4);
+        for (int i = tid; i < words; i += blockDim.x) dst[i] = src[i];
+    }
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&done[s], NC);
+        }
+        abort_flag = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int64_t ntiles = P.ntiles;
+    const int64_t first = blockIdx.x, stride = gridDim.x;
+    const int64_t nmine = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;
+
+    if (tid >= NC) {
+        // ------------------------------------------------------------ producer warp
+        const int lane = tid & 31;
+        const int lo = P.lo;
+        const int rank = P.tma_rank;
+        auto coords = [&](int64_t T, int32_t *c) {
+            int pos = 0;
+            for (int d = 0; d < rank; d++) {
+                const int f = P.tdim_free[d];
+                c[d] = (int32_t)(((T >> pos) & ((1ll << f) - 1)) << P.tdim_box[d]);
+                pos += f;
+            }
+        };
+        const int nsub = 1 << (KW - lo);
+        const uint32_t subbytes = 8u << lo;
+        const int nh = P.nh;
+        auto tile_base = [&](int64_t T) -> int64_t {
+            int64_t x = T << lo;                      // free bits are the bits outside [0, lo) U H
+            for (int i = 0; i < nh; i++) {
+                const int h = P.H[i];
+                x = ((x >> h) << (h + 1)) | (x & ((1ll << h) - 1));
+            }
+            return x;
+        };
+        auto sub_off = [&](int s) -> int64_t {
+            int64_t o = 0;
+            for (int i = 0; i < KW - lo; i++)
+                if ((s >> i) & 1) o |= 1ll << P.H[i];
+            return o;
+        };
+        auto issue_load = [&](int64_t j, int b) {
+            const int64_t T = first + j * stride;
+            float2 *dst = bufs + (size_t)b * TILE;
+            if (rank) {
+                if (lane == 0) {
+                    int32_t c[QSV_TMA_MAX_RANK];
+                    coords(T, c);
+                    mbar_arrive_expect_tx(&full[b], (uint32_t)TILE * 8u);
+                    tma_load(dst, tmap, c, rank, &full[b]);
+                }
+                return;
+            }
+            const int64_t base = tile_base(T);
+            if (lane == 0) mbar_arrive_expect_tx(&full[b], (uint32_t)TILE * 8u);
+            __syncwarp();
+            for (int s = lane; s < nsub; s += 32) bulk_g2s(dst + (s << lo), state + (base | sub_off(s)), subbytes, &full[b]);
+        };
+        auto issue_store = [&](int64_t j, int b) {
+            const int64_t T = first + j * stride;
+            const float2 *src = bufs + (size_t)b * TILE;
+            if (rank) {
+                if (lane == 0) {
+                    int32_t c[QSV_TMA_MAX_RANK];
+                    coords(T, c);
+                    tma_store(tmap, c, rank, src);
+                    bulk_commit();
+                }
+                return;
+            }
+            const int64_t base = tile_base(T);
+            for (int s = lane; s < nsub; s += 32) bulk_s2g(state + (base | sub_off(s)), src + (s << lo), subbytes);
+            bulk_commit();
+        };
+        for (int64_t j = 0; j < S && j < nmine; j++) issue_load(j, (int)j);
+        for (int64_t j = 0; j < nmine; j++) {
+            const int b = (int)(j % S);
+            const uint32_t par = (uint32_t)((j / S) & 1);
+            if (!mbar_wait(&done[b], par, &abort_flag, status)) break;
+            issue_store(j, b);
+            if (j + S < nmine) {
+                bulk_wait_read_all();                 // this lane's stores have read the buffer
+                __syncwarp();
+                issue_load(j + S, b);
+            }
+        }
+        bulk_wait_all();
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumer warps
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int64_t j = 0; j < nmine; j++) {
+        const int b = (int)(j % S);
+        const uint32_t par = (uint32_t)((j / S) & 1);
+        if (!mbar_wait(&full[b], par, &abort_flag, status)) break;
+        float2 *tile = bufs + (size_t)b * TILE;
+        Body::template tile<NV, RB, WB>(tile, P, sops, lane, warp);
+        fence_proxy_async_smem();
+        mbar_arrive(&done[b]);
+    }
+}
+
+}  // namespace dev
+}  // namespace qsv

@@ -66,6 +66,10 @@ def load(path=LIB_PATH):
         "qsv_batch_upload": ([P, P, SZ, P], I32),
         "qsv_batch_launch": ([P, P, SZ, P], I32),
         "qsv_set_phase_lanes": ([ctypes.c_int], I32),
+        "qsv_set_jit": ([ctypes.c_int], I32),
+        "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
+        "qsv_jit_wait": ([], I32),
+        "qsv_jit_info": ([P, ctypes.c_int], I32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -82,7 +86,8 @@ def exported_symbols():
             "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
             "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
-            "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch"]
+            "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
+            "qsv_jit_wait", "qsv_jit_info"]
 
 
 def _check(rc):
@@ -294,3 +299,38 @@ def set_layout13(rb):
 
 def set_phase_lanes(k):
     _check(load().qsv_set_phase_lanes(int(k)))
+
+
+JIT_MODES = {"off": 0, "eager": 1, "auto": 2}
+
+
+def set_jit(mode):
+    """Specialised sweep kernels: "off" (interpreter only), "eager" (compile each new sweep structure before
+    its first launch) or "auto" (default: compile in the background once a structure repeats). Values are
+    identical in every mode. Returns the previous mode's name."""
+    rc = load().qsv_set_jit(JIT_MODES[mode] if isinstance(mode, str) else int(mode))
+    if rc < 0:
+        _check(rc)
+    return {v: k for k, v in JIT_MODES.items()}[rc]
+
+
+def jit_prepare(seg, n):
+    """Compile (blocking, in parallel) the specialised kernels of every sweep of a segment. Host only.
+    Returns the number of the segment's sweep structures whose kernel is ready."""
+    w = np.ascontiguousarray(seg, dtype=np.int32)
+    rc = load().qsv_jit_prepare(w.ctypes.data_as(ctypes.c_void_p), w.size, int(n))
+    if rc < 0:
+        _check(rc)
+    return rc
+
+
+def jit_wait():
+    _check(load().qsv_jit_wait())
+
+
+def jit_info():
+    """Counters of the specialised-kernel cache."""
+    buf = (ctypes.c_longlong * 8)()
+    load().qsv_jit_info(ctypes.cast(buf, ctypes.c_void_p), 8)
+    keys = ["mode", "structures", "ready", "failed", "jit_launches", "interp_launches", "compile_ms", "pending"]
+    return dict(zip(keys, [int(x) for x in buf]))
