@@ -11,7 +11,30 @@ from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
+def _qubit0_controls(n, seed):
+    """Controlled gates with qubit 0 as control (targets on every other qubit) and as target, plus dense
+    layers: exercises tile-bit-0 ops of every kind and controls on tile bit 0 for register and lane targets."""
+    rng = np.random.default_rng(seed)
+    qc = gen.random_layer(n, 1, seed)
+    for t in range(1, n):
+        th = float(rng.uniform(-np.pi, np.pi))
+        qc.cx(0, t)
+        qc.cz(0, t)
+        qc.ch(0, t)
+        qc.crx(th, 0, t)
+        qc.cp(th, 0, t)
+        qc.cx(t, 0)
+        qc.ch(t, 0)
+        qc.crz(th, t, 0)
+        qc.u(th, th / 3, -th / 2, t)
+    qc.ccx(0, 1, n - 1)
+    qc.ccx(n - 1, 0, 2)
+    return qc
+
+
 CASES = [
+    (14, 12, lambda: _qubit0_controls(14, 1)),
+    (19, 12, lambda: _qubit0_controls(19, 2)),
     (10, 8, lambda: gen.random_layer(10, 6, 11)),
     (11, 9, lambda: gen.random_layer_ccx(11, 5, 12)),
     (12, 12, lambda: gen.zoo(12, 3)),

@@ -120,6 +120,7 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
     for (int o = 0; o < sw.nops; o++) {
         const QsvOp &op = sw.ops[o];
         put(op.slot); put(op.variant); put(op.cm_reg); put32(op.cm_thr);
+        put(op.kind); put(op.cls0); put(op.cls1); put(op.cm_c);
     }
     return k;
 }
@@ -146,14 +147,25 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
         for (int o = ph.op_begin; o < ph.op_end; o++) {
             const QsvOp &op = sw.ops[o];
             const std::string thr = std::to_string(op.cm_thr) + "u";
+            const std::string cls = std::to_string((int)op.kind) + ", " + std::to_string((int)op.cls0) + ", " +
+                                    std::to_string((int)op.cls1) + ", ";
+            const std::string ctl = std::to_string((int)op.cm_reg) + ", " + thr;
+            const std::string mux = std::to_string((int)op.kind) + ", " + std::to_string((int)op.cls1) + ", " +
+                                    std::to_string((int)op.cm_c) + ", " + ctl;
             if (op.slot == QSV_SLOT_COMP)
-                s << "            jit_comp<NV, " << thr << ">(R, I, P.ops[" << o << "], tb);\n";
+                s << "            jit_comp<NV, " << cls << ctl << ">(R, I, P.ops[" << o << "], tb);\n";
+            else if (op.slot < QSV_SLOT_LANE0 && op.variant == QSV_V_MUX)
+                s << "            jit_reg_mux<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << mux << ">(R, I, P.ops[" << o
+                  << "], tb);\n";
             else if (op.slot < QSV_SLOT_LANE0)
-                s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << (int)op.variant << ", "
-                  << (int)op.cm_reg << ", " << thr << ">(R, I, P.ops[" << o << "], tb);\n";
+                s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << (int)op.variant << ", " << ctl
+                  << ">(R, I, P.ops[" << o << "], tb);\n";
+            else if (op.variant == QSV_V_MUX)
+                s << "            jit_lane_mux<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << mux << ">(R, I, P.ops["
+                  << o << "], tb, lane);\n";
             else
-                s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", "
-                  << (int)op.cm_reg << ", " << thr << ">(R, I, P.ops[" << o << "], tb, lane);\n";
+                s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", " << ctl
+                  << ">(R, I, P.ops[" << o << "], tb, lane);\n";
         }
         s << "            jit_store<NV, " << rbits << ">(tile, tb, R, I);\n        }\n";
     }

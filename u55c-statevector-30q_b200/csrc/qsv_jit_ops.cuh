@@ -226,13 +226,147 @@ __device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const
 }
 
 // ---------------------------------------------------------------- tile-bit-0 target (halves of a float4)
-template <int NV, uint32_t CMTHR>
+// the interpreter's comp_op with kind, classes and register controls fixed at compile time
+template <int CLS>
+__device__ __forceinline__ void jit_pair(float &x0r, float &x0i, float &x1r, float &x1i, const float *m) {
+    if constexpr (CLS == QSV_M_DENSE) {
+        float y0r, y0i, y1r, y1i;
+        lin_own(y0r, y0i, m[0], m[1], m[2], m[3], x0r, x0i, x1r, x1i);
+        lin_own(y1r, y1i, m[6], m[7], m[4], m[5], x1r, x1i, x0r, x0i);
+        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_DIAG) {
+        float y0r, y0i, y1r, y1i;
+        diag_own(y0r, y0i, m[0], m[1], x0r, x0i);
+        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
+        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_DIAG1) {
+        float y1r, y1i;
+        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
+        x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_XSWAP) {
+        float t = x0r; x0r = x1r; x1r = t;
+        t = x0i; x0i = x1i; x1i = t;
+    }
+}
+
+template <int NV, int KIND, int CLS0, int CLS1, int CMREG, uint32_t CMTHR>
 __device__ __forceinline__ void jit_comp(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
     const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
     float m0[8], m1[8];
     jit_mat(m0, op.m0);
     jit_mat(m1, op.m1);
-    comp_op<NV>(R, I, op, m0, m1, tok);
+#pragma unroll
+    for (int r = 0; r < NV; r++) {
+        constexpr bool UNI = KIND == QSV_K_UNI, CTRL = KIND == QSV_K_CTRL;
+        const bool regsel = !UNI && (r & CMREG) == CMREG;
+        if (CTRL && !regsel) continue;
+        float x0r = R[r].x, x0i = I[r].x, x1r = R[r].y, x1i = I[r].y;
+        if (UNI) {
+            jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+        } else if (CMTHR == 0u) {
+            if (regsel) jit_pair<CLS1>(x0r, x0i, x1r, x1i, m1);
+            else jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+        } else {
+            if (regsel && tok) jit_pair<CLS1>(x0r, x0i, x1r, x1i, m1);
+            else if (!CTRL) jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+        }
+        R[r] = make_float2(x0r, x1r);
+        I[r] = make_float2(x0i, x1i);
+    }
+}
+
+// ---------------------------------------------------------------- controlled ops with a control on tile bit 0
+// M0 = identity and tile bit 0 among the controls: only the bit-0 = 1 half of each float4 (the .y lanes of
+// the packed pairs) can be selected. XSWAP / DIAG1 / DENSE M1 in scalar arithmetic on that half; other
+// matrices take the interpreter's general path.
+template <int NV, int RBIT, int CLS1, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ bool jit_reg_ctrl_c(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
+    constexpr int B = 1 << RBIT;
+    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
+    if constexpr (CLS1 == QSV_M_XSWAP) {
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & B) || (r & CMREG) != CMREG) continue;
+            const float a = R[r].y, b = R[r | B].y, c = I[r].y, d = I[r | B].y;
+            R[r].y = tok ? b : a; R[r | B].y = tok ? a : b;
+            I[r].y = tok ? d : c; I[r | B].y = tok ? c : d;
+        }
+        return true;
+    } else if constexpr (CLS1 == QSV_M_DIAG1 || CLS1 == QSV_M_DENSE || CLS1 == QSV_M_DIAG) {
+        float m[8];
+        jit_mat(m, op.m1);
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & B) || (r & CMREG) != CMREG) continue;
+            float x0r = R[r].y, x0i = I[r].y, x1r = R[r | B].y, x1i = I[r | B].y;
+            jit_pair<CLS1>(x0r, x0i, x1r, x1i, m);
+            R[r].y = tok ? x0r : R[r].y; I[r].y = tok ? x0i : I[r].y;
+            R[r | B].y = tok ? x1r : R[r | B].y; I[r | B].y = tok ? x1i : I[r | B].y;
+        }
+        return true;
+    }
+    return false;
+}
+
+template <int NV, int LB, int CLS1, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ bool jit_lane_ctrl_c(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb,
+                                                int lane) {
+    constexpr int XM = 1 << LB;
+    const bool mine = (lane >> LB) & 1;
+    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
+    if constexpr (CLS1 == QSV_M_XSWAP) {
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & CMREG) != CMREG) continue;
+            const float oR = __shfl_xor_sync(0xffffffffu, R[r].y, XM);
+            const float oI = __shfl_xor_sync(0xffffffffu, I[r].y, XM);
+            R[r].y = tok ? oR : R[r].y;
+            I[r].y = tok ? oI : I[r].y;
+        }
+        return true;
+    } else if constexpr (CLS1 == QSV_M_DIAG1) {
+        const bool s = mine && tok;
+        const float d_r = op.m1[6], d_i = op.m1[7];
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & CMREG) != CMREG) continue;
+            float yr, yi;
+            diag_own(yr, yi, d_r, d_i, R[r].y, I[r].y);
+            R[r].y = s ? yr : R[r].y;
+            I[r].y = s ? yi : I[r].y;
+        }
+        return true;
+    } else if constexpr (CLS1 == QSV_M_DENSE || CLS1 == QSV_M_DIAG) {
+        const float *m = op.m1;
+        const float a_r = mine ? m[6] : m[0], a_i = mine ? m[7] : m[1];
+        const float b_r = mine ? m[4] : m[2], b_i = mine ? m[5] : m[3];
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & CMREG) != CMREG) continue;
+            const float oR = __shfl_xor_sync(0xffffffffu, R[r].y, XM);
+            const float oI = __shfl_xor_sync(0xffffffffu, I[r].y, XM);
+            float yr, yi;
+            lin_own(yr, yi, a_r, a_i, b_r, b_i, R[r].y, I[r].y, oR, oI);
+            R[r].y = tok ? yr : R[r].y;
+            I[r].y = tok ? yi : I[r].y;
+        }
+        return true;
+    }
+    return false;
+}
+
+template <int NV, int RBIT, int KIND, int CLS1, int CMC, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ void jit_reg_mux(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
+    if constexpr (KIND == QSV_K_CTRL && CMC)
+        if (jit_reg_ctrl_c<NV, RBIT, CLS1, CMREG, CMTHR>(R, I, op, tb)) return;
+    jit_reg<NV, RBIT, QSV_V_MUX, CMREG, CMTHR>(R, I, op, tb);
+}
+
+template <int NV, int LB, int KIND, int CLS1, int CMC, int CMREG, uint32_t CMTHR>
+__device__ __forceinline__ void jit_lane_mux(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb, int lane) {
+    if constexpr (KIND == QSV_K_CTRL && CMC)
+        if (jit_lane_ctrl_c<NV, LB, CLS1, CMREG, CMTHR>(R, I, op, tb, lane)) return;
+    jit_lane<NV, LB, QSV_V_MUX, CMREG, CMTHR>(R, I, op, tb, lane);
 }
 
 }  // namespace dev
