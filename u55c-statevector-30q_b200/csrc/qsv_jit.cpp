@@ -47,6 +47,17 @@ constexpr int kThreshold = 2;      // launches of a structure before automatic m
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
 
+// consumer groups per CTA. One by default; QSV_JIT_GROUPS13=2 gives 13-qubit windows with 8-warp groups
+// two groups taking alternate tiles (16 consumer warps, registers capped near 96 per thread). Measured on
+// the 30-qubit random-layer and QFT programs, two groups were no faster than one.
+int groups_for(int kw, int wb) {
+    static const int g13 = [] {
+        const char *e = std::getenv("QSV_JIT_GROUPS13");
+        return e && std::atoi(e) == 2 ? 2 : 1;
+    }();
+    return kw == 13 && wb <= 3 ? g13 : 1;
+}
+
 struct Drv {
     PFN_cuModuleLoadData_v2000 module_load = nullptr;
     PFN_cuModuleGetFunction_v2000 get_function = nullptr;
@@ -127,16 +138,18 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
 
 // CUDA source of the kernel specialised to sw's structure
 std::string gen_source(const QsvSweep &sw, int rb, int wb) {
-    const int nc = 1 << (5 + wb), nt = nc + 32, minb = sw.kw >= 13 ? 1 : 2;
+    const int groups = groups_for(sw.kw, wb);
+    const int nc = 1 << (5 + wb), nt = groups * nc + 32, minb = sw.kw >= 13 ? 1 : 2;
     std::ostringstream s;
     s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
       << "namespace qsv {\nnamespace dev {\nstruct JitBody {\n"
       << "    static constexpr bool kSmemOps = false;\n"
       << "    template <int NV, int RB, int WB>\n"
-      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *, int lane, int warp) {\n";
+      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *, int lane, int warp,\n"
+      << "                                                int bar) {\n";
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
-        if (p > 0) s << "        named_bar_sync(1, " << nc << ");\n";
+        if (p > 0) s << "        named_bar_sync(bar, " << nc << ");\n";
         s << "        {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_bits[0] << ", "
           << (int)ph.lane_bits[1] << ">(lane)";
         for (int w = 0; w < wb; w++) s << " | jit_warp_bit<" << (int)ph.warp_bits[w] << ">(warp, " << w << ")";
@@ -173,7 +186,7 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
       << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb << ")\n"
       << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
       << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
-      << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages
+      << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages << ", " << groups
       << ", qsv::dev::JitBody>(state, P, &tmap, status);\n}\n";
     return s.str();
 }
@@ -342,7 +355,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
-    const int NT = (1 << (5 + wb)) + 32;
+    const int NT = groups_for(sw.kw, wb) * (1 << (5 + wb)) + 32;
     const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2);
     if (!e->fn[dev]) {
         // loading a module is not a stream operation: keep it out of stream captures

@@ -31,10 +31,11 @@ __device__ int g_status = 0;
 struct InterpBody {
     static constexpr bool kSmemOps = true;
     template <int NV, int RB, int WB>
-    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane, int warp) {
+    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane, int warp,
+                                                int bar) {
         constexpr int NC = 1 << (5 + WB);
         for (int ph = 0; ph < P.nphases; ph++) {
-            if (ph > 0) named_bar_sync(1, NC);
+            if (ph > 0) named_bar_sync(bar, NC);
             const QsvPhase &Q = P.phases[ph];
             run_phase<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp);
         }
@@ -44,7 +45,7 @@ struct InterpBody {
 template <int KW, int RB, int WB, int S>
 __global__ void __launch_bounds__((1 << (5 + WB)) + 32, (KW >= 13 ? 1 : 2))
     sweep_kernel(float2 *__restrict__ state, const __grid_constant__ QsvSweep P, const __grid_constant__ CUtensorMap tmap) {
-    sweep_pipeline<KW, RB, WB, S, InterpBody>(state, P, &tmap, &g_status);
+    sweep_pipeline<KW, RB, WB, S, 1, InterpBody>(state, P, &tmap, &g_status);
 }
 
 // ---------------------------------------------------------------- host launchers

@@ -5,7 +5,9 @@
 //   * a producer warp streams tiles HBM -> shared memory and back with the TMA engine: one tensor-map box
 //     per tile when the window's contiguous runs are short, one bulk-async copy per sub-block when they
 //     are long; completion is counted on mbarriers, up to S tiles are in flight;
-//   * consumer warps run Body::tile on each staged tile (the ops of the sweep, in registers).
+//   * G groups of consumer warps run Body::tile on the staged tiles (the ops of the sweep, in registers);
+//     with G = 2 the groups take alternate tiles, so one group's phase barriers and shared-memory round
+//     trips overlap the other group's arithmetic.
 // Body is the interpreter (qsv_sweep.cu: op table read at run time) or a kernel specialised to one sweep
 // structure (qsv_jit.cpp: ops fixed at compile time). Both run the same arithmetic (qsv_ops.cuh).
 // The tile addressing is the reference's (host/sv/model.py:25-40, sv_engine.cpp:61-84,116): tile T's
@@ -68,12 +70,13 @@ __host__ __device__ constexpr size_t sweep_smem_bytes(bool smem_ops) {
     return ((size_t)S << KW) * 8 + (smem_ops ? sizeof(QsvOp) * QSV_MAX_SWEEP_OPS : 0);
 }
 
-// The pipeline. Launch with (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S>(Body::kSmemOps) bytes
-// of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
-template <int KW, int RB, int WB, int S, class Body>
+// The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S>(Body::kSmemOps)
+// bytes of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
+template <int KW, int RB, int WB, int S, int G, class Body>
 __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const QsvSweep &P, const CUtensorMap *tmap,
                                                int *status) {
-    constexpr int NC = 1 << (5 + WB);        // consumer threads
+    constexpr int NCG = 1 << (5 + WB);       // consumer threads of one group
+    constexpr int NC = G * NCG;              // consumer threads
     constexpr int NV = 1 << RB;              // float4 per consumer thread
     constexpr int TILE = 1 << KW;            // amplitudes per tile
     static_assert(1 + 3 + 2 + RB + WB == KW, "layout must cover the window");
@@ -82,7 +85,11 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
     // the interpreter's op table, copied once from the parameter block: shared-memory reads of an op's
     // fields are independent short-latency loads (the constant-bank path serialises run-time indices)
     QsvOp *sops = reinterpret_cast<QsvOp *>(smem_raw + ((size_t)S << KW) * sizeof(float2));
-    __shared__ __align__(8) uint64_t full[S];
+    // full barrier of tile j: full[j % (S * G)]. Tiles sharing a full barrier share a buffer (j % S) and a
+    // consumer group (j % G), so each full barrier is waited on by one group, phase after phase (a parity
+    // wait never meets a phase two steps old). done[b] is waited on by the producer alone, tile by tile.
+    constexpr int NF = S * G;
+    __shared__ __align__(8) uint64_t full[NF];
     __shared__ __align__(8) uint64_t done[S];
     __shared__ volatile int abort_flag;
 
@@ -94,10 +101,8 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
         for (int i = tid; i < words; i += blockDim.x) dst[i] = src[i];
     }
     if (tid == 0) {
-        for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], 1);
-            mbar_init(&done[s], NC);
-        }
+        for (int f = 0; f < NF; f++) mbar_init(&full[f], 1);
+        for (int s = 0; s < S; s++) mbar_init(&done[s], NCG);
         abort_flag = 0;
         fence_mbar_init();
     }
@@ -140,19 +145,20 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
         auto issue_load = [&](int64_t j, int b) {
             const int64_t T = first + j * stride;
             float2 *dst = bufs + (size_t)b * TILE;
+            uint64_t *fb = &full[j % NF];
             if (rank) {
                 if (lane == 0) {
                     int32_t c[QSV_TMA_MAX_RANK];
                     coords(T, c);
-                    mbar_arrive_expect_tx(&full[b], (uint32_t)TILE * 8u);
-                    tma_load(dst, tmap, c, rank, &full[b]);
+                    mbar_arrive_expect_tx(fb, (uint32_t)TILE * 8u);
+                    tma_load(dst, tmap, c, rank, fb);
                 }
                 return;
             }
             const int64_t base = tile_base(T);
-            if (lane == 0) mbar_arrive_expect_tx(&full[b], (uint32_t)TILE * 8u);
+            if (lane == 0) mbar_arrive_expect_tx(fb, (uint32_t)TILE * 8u);
             __syncwarp();
-            for (int s = lane; s < nsub; s += 32) bulk_g2s(dst + (s << lo), state + (base | sub_off(s)), subbytes, &full[b]);
+            for (int s = lane; s < nsub; s += 32) bulk_g2s(dst + (s << lo), state + (base | sub_off(s)), subbytes, fb);
         };
         auto issue_store = [&](int64_t j, int b) {
             const int64_t T = first + j * stride;
@@ -187,13 +193,14 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
     }
 
     // ---------------------------------------------------------------- consumer warps
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int64_t j = 0; j < nmine; j++) {
+    const int grp = tid / NCG;                   // group grp takes tiles grp, grp + G, ...
+    const int lane = tid & 31, warp = (tid % NCG) >> 5;
+    for (int64_t j = grp; j < nmine; j += G) {
         const int b = (int)(j % S);
-        const uint32_t par = (uint32_t)((j / S) & 1);
-        if (!mbar_wait(&full[b], par, &abort_flag, status)) break;
+        const uint32_t par = (uint32_t)((j / NF) & 1);
+        if (!mbar_wait(&full[j % NF], par, &abort_flag, status)) break;
         float2 *tile = bufs + (size_t)b * TILE;
-        Body::template tile<NV, RB, WB>(tile, P, sops, lane, warp);
+        Body::template tile<NV, RB, WB>(tile, P, sops, lane, warp, 1 + grp);
         fence_proxy_async_smem();
         mbar_arrive(&done[b]);
     }
