@@ -136,29 +136,8 @@ __device__ __forceinline__ void jit_reg(float2 (&R)[NV], float2 (&I)[NV], const 
 }
 
 // ---------------------------------------------------------------- lane-bit target (LB = lane bit 0..4)
-// For an output amplitude "own" with partner "oth" on lane ^ (1 << LB): y = a*own + b*oth, (a, b) =
-// (m00, m01) on the bit-0 side and (m11, m10) on the bit-1 side -- the interpreter's lane update.
-__device__ __forceinline__ void jit_lane_lin(float2 &R, float2 &I, const float2 oR, const float2 oI, const float2 ar,
-                                             const float2 ai, const float2 nai, const float2 br, const float2 bi,
-                                             const float2 nbi) {
-    float2 t = __fmul2_rn(nbi, oI);
-    t = __ffma2_rn(br, oR, t);
-    t = __ffma2_rn(nai, I, t);
-    const float2 yr = __ffma2_rn(ar, R, t);
-    float2 u = __fmul2_rn(bi, oR);
-    u = __ffma2_rn(br, oI, u);
-    u = __ffma2_rn(ai, R, u);
-    const float2 yi = __ffma2_rn(ar, I, u);
-    R = yr;
-    I = yi;
-}
-__device__ __forceinline__ void jit_shfl(const float2 &R, const float2 &I, float2 &oR, float2 &oI, int xm) {
-    oR.x = __shfl_xor_sync(0xffffffffu, R.x, xm);
-    oR.y = __shfl_xor_sync(0xffffffffu, R.y, xm);
-    oI.x = __shfl_xor_sync(0xffffffffu, I.x, xm);
-    oI.y = __shfl_xor_sync(0xffffffffu, I.y, xm);
-}
-
+// lane updates use lane_lin / shfl4 (qsv_ops.cuh): y = a*own + b*oth, (a, b) = (m00, m01) on the bit-0
+// side and (m11, m10) on the bit-1 side -- the interpreter's lane update.
 template <int NV, int LB, int VAR, int CMREG, uint32_t CMTHR>
 __device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb, int lane) {
     constexpr int XM = 1 << LB;
@@ -176,9 +155,9 @@ __device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const
         for (int r = 0; r < NV; r++) {
             if (!UNI && (r & CMREG) != CMREG) continue;
             float2 oR, oI;
-            jit_shfl(R[r], I[r], oR, oI, XM);
+            shfl4(R[r], I[r], oR, oI, XM);
             float2 yR = R[r], yI = I[r];
-            jit_lane_lin(yR, yI, oR, oI, ar, ai, nai, br, bi, nbi);
+            lane_lin(yR, yI, oR, oI, ar, ai, nai, br, bi, nbi);
             if (UNI || CMTHR == 0u) {
                 R[r] = yR; I[r] = yI;
             } else {
@@ -209,7 +188,7 @@ __device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const
         for (int r = 0; r < NV; r++) {
             if (!UNI && (r & CMREG) != CMREG) continue;
             float2 oR, oI;
-            jit_shfl(R[r], I[r], oR, oI, XM);
+            shfl4(R[r], I[r], oR, oI, XM);
             if (UNI || CMTHR == 0u) {
                 R[r] = oR; I[r] = oI;
             } else {
@@ -226,29 +205,8 @@ __device__ __forceinline__ void jit_lane(float2 (&R)[NV], float2 (&I)[NV], const
 }
 
 // ---------------------------------------------------------------- tile-bit-0 target (halves of a float4)
-// the interpreter's comp_op with kind, classes and register controls fixed at compile time
-template <int CLS>
-__device__ __forceinline__ void jit_pair(float &x0r, float &x0i, float &x1r, float &x1i, const float *m) {
-    if constexpr (CLS == QSV_M_DENSE) {
-        float y0r, y0i, y1r, y1i;
-        lin_own(y0r, y0i, m[0], m[1], m[2], m[3], x0r, x0i, x1r, x1i);
-        lin_own(y1r, y1i, m[6], m[7], m[4], m[5], x1r, x1i, x0r, x0i);
-        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
-    } else if constexpr (CLS == QSV_M_DIAG) {
-        float y0r, y0i, y1r, y1i;
-        diag_own(y0r, y0i, m[0], m[1], x0r, x0i);
-        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
-        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
-    } else if constexpr (CLS == QSV_M_DIAG1) {
-        float y1r, y1i;
-        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
-        x1r = y1r; x1i = y1i;
-    } else if constexpr (CLS == QSV_M_XSWAP) {
-        float t = x0r; x0r = x1r; x1r = t;
-        t = x0i; x0i = x1i; x1i = t;
-    }
-}
-
+// the interpreter's comp_op with kind, classes and register controls fixed at compile time (pair_t:
+// pair_apply with the class fixed, qsv_ops.cuh)
 template <int NV, int KIND, int CLS0, int CLS1, int CMREG, uint32_t CMTHR>
 __device__ __forceinline__ void jit_comp(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, uint32_t tb) {
     const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
@@ -262,13 +220,13 @@ __device__ __forceinline__ void jit_comp(float2 (&R)[NV], float2 (&I)[NV], const
         if (CTRL && !regsel) continue;
         float x0r = R[r].x, x0i = I[r].x, x1r = R[r].y, x1i = I[r].y;
         if (UNI) {
-            jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+            pair_t<CLS0>(x0r, x0i, x1r, x1i, m0);
         } else if (CMTHR == 0u) {
-            if (regsel) jit_pair<CLS1>(x0r, x0i, x1r, x1i, m1);
-            else jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+            if (regsel) pair_t<CLS1>(x0r, x0i, x1r, x1i, m1);
+            else pair_t<CLS0>(x0r, x0i, x1r, x1i, m0);
         } else {
-            if (regsel && tok) jit_pair<CLS1>(x0r, x0i, x1r, x1i, m1);
-            else if (!CTRL) jit_pair<CLS0>(x0r, x0i, x1r, x1i, m0);
+            if (regsel && tok) pair_t<CLS1>(x0r, x0i, x1r, x1i, m1);
+            else if (!CTRL) pair_t<CLS0>(x0r, x0i, x1r, x1i, m0);
         }
         R[r] = make_float2(x0r, x1r);
         I[r] = make_float2(x0i, x1i);
@@ -299,7 +257,7 @@ __device__ __forceinline__ bool jit_reg_ctrl_c(float2 (&R)[NV], float2 (&I)[NV],
         for (int r = 0; r < NV; r++) {
             if ((r & B) || (r & CMREG) != CMREG) continue;
             float x0r = R[r].y, x0i = I[r].y, x1r = R[r | B].y, x1i = I[r | B].y;
-            jit_pair<CLS1>(x0r, x0i, x1r, x1i, m);
+            pair_t<CLS1>(x0r, x0i, x1r, x1i, m);
             R[r].y = tok ? x0r : R[r].y; I[r].y = tok ? x0i : I[r].y;
             R[r | B].y = tok ? x1r : R[r | B].y; I[r | B].y = tok ? x1i : I[r | B].y;
         }

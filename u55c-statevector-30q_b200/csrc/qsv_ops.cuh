@@ -192,6 +192,203 @@ __device__ __forceinline__ void lane_op(float2 (&R)[NV], float2 (&I)[NV], const 
     }
 }
 
+// ---------------------------------------------------------------- shared building blocks
+// lane update y = a*own + b*oth on two packed pairs (the lane_op arithmetic with hoisted coefficients)
+__device__ __forceinline__ void lane_lin(float2 &R, float2 &I, const float2 oR, const float2 oI, const float2 ar,
+                                         const float2 ai, const float2 nai, const float2 br, const float2 bi,
+                                         const float2 nbi) {
+    float2 t = __fmul2_rn(nbi, oI);
+    t = __ffma2_rn(br, oR, t);
+    t = __ffma2_rn(nai, I, t);
+    const float2 yr = __ffma2_rn(ar, R, t);
+    float2 u = __fmul2_rn(bi, oR);
+    u = __ffma2_rn(br, oI, u);
+    u = __ffma2_rn(ai, R, u);
+    const float2 yi = __ffma2_rn(ar, I, u);
+    R = yr;
+    I = yi;
+}
+__device__ __forceinline__ void shfl4(const float2 &R, const float2 &I, float2 &oR, float2 &oI, int xm) {
+    oR.x = __shfl_xor_sync(0xffffffffu, R.x, xm);
+    oR.y = __shfl_xor_sync(0xffffffffu, R.y, xm);
+    oI.x = __shfl_xor_sync(0xffffffffu, I.x, xm);
+    oI.y = __shfl_xor_sync(0xffffffffu, I.y, xm);
+}
+// pair_apply with the matrix class fixed at compile time
+template <int CLS>
+__device__ __forceinline__ void pair_t(float &x0r, float &x0i, float &x1r, float &x1i, const float *m) {
+    if constexpr (CLS == QSV_M_DENSE) {
+        float y0r, y0i, y1r, y1i;
+        lin_own(y0r, y0i, m[0], m[1], m[2], m[3], x0r, x0i, x1r, x1i);
+        lin_own(y1r, y1i, m[6], m[7], m[4], m[5], x1r, x1i, x0r, x0i);
+        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_DIAG) {
+        float y0r, y0i, y1r, y1i;
+        diag_own(y0r, y0i, m[0], m[1], x0r, x0i);
+        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
+        x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_DIAG1) {
+        float y1r, y1i;
+        diag_own(y1r, y1i, m[6], m[7], x1r, x1i);
+        x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_XSWAP) {
+        float t = x0r; x0r = x1r; x1r = t;
+        t = x0i; x0i = x1i; x1i = t;
+    }
+}
+
+// ---------------------------------------------------------------- one dispatch per op
+// The interpreter's fast paths: a uniform switch per op selects a tight loop (coefficients hoisted, no
+// per-pair selects). Same values as comp_op / lane_op (forms that skip work skip exact-zero terms or
+// unselected pairs only).
+template <int NV, int CLS, bool CTRL>
+__device__ __forceinline__ void comp_loop(float2 (&R)[NV], float2 (&I)[NV], const float *m, int cm_reg, bool tok) {
+#pragma unroll
+    for (int r = 0; r < NV; r++) {
+        if (CTRL && !(tok && (r & cm_reg) == cm_reg)) continue;
+        float x0r = R[r].x, x0i = I[r].x, x1r = R[r].y, x1i = I[r].y;
+        pair_t<CLS>(x0r, x0i, x1r, x1i, m);
+        R[r] = make_float2(x0r, x1r);
+        I[r] = make_float2(x0i, x1i);
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, const float *m0,
+                                             const float *m1, bool tok) {
+    const int cm_reg = op.cm_reg;
+    if (op.kind == QSV_K_UNI) {
+        switch (op.cls0) {
+            case QSV_M_DENSE: comp_loop<NV, QSV_M_DENSE, false>(R, I, m0, 0, true); return;
+            case QSV_M_DIAG: comp_loop<NV, QSV_M_DIAG, false>(R, I, m0, 0, true); return;
+            case QSV_M_DIAG1: comp_loop<NV, QSV_M_DIAG1, false>(R, I, m0, 0, true); return;
+            case QSV_M_XSWAP: comp_loop<NV, QSV_M_XSWAP, false>(R, I, m0, 0, true); return;
+            case QSV_M_IDENT: return;
+            default: break;
+        }
+    } else if (op.kind == QSV_K_CTRL) {
+        switch (op.cls1) {
+            case QSV_M_DENSE: comp_loop<NV, QSV_M_DENSE, true>(R, I, m1, cm_reg, tok); return;
+            case QSV_M_DIAG: comp_loop<NV, QSV_M_DIAG, true>(R, I, m1, cm_reg, tok); return;
+            case QSV_M_DIAG1: comp_loop<NV, QSV_M_DIAG1, true>(R, I, m1, cm_reg, tok); return;
+            case QSV_M_XSWAP: comp_loop<NV, QSV_M_XSWAP, true>(R, I, m1, cm_reg, tok); return;
+            case QSV_M_IDENT: return;
+            default: break;
+        }
+    }
+    comp_op<NV>(R, I, op, m0, m1, tok);
+}
+
+template <int NV>
+__device__ __forceinline__ void lane_op_fast(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, const float *m0,
+                                             const float *m1, bool tok, int lanebit, int lane) {
+    const int xm = 1 << lanebit;
+    const bool mine = (lane >> lanebit) & 1;
+    const int cm_reg = op.cm_reg;
+    const int var = op.variant;
+    if (var == QSV_V_UNI_DENSE || var == QSV_V_CTRL_DENSE || var == QSV_V_CTRL_DENSE_SEL) {
+        const bool uni = var == QSV_V_UNI_DENSE;
+        const float *m = uni ? m0 : m1;
+        const float a_r = mine ? m[6] : m[0], a_i = mine ? m[7] : m[1];
+        const float b_r = mine ? m[4] : m[2], b_i = mine ? m[5] : m[3];
+        const float2 ar = f2(a_r), ai = f2(a_i), nai = f2(-a_i), br = f2(b_r), bi = f2(b_i), nbi = f2(-b_i);
+        if (uni) {
+#pragma unroll
+            for (int r = 0; r < NV; r++) {
+                float2 oR, oI;
+                shfl4(R[r], I[r], oR, oI, xm);
+                lane_lin(R[r], I[r], oR, oI, ar, ai, nai, br, bi, nbi);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < NV; r++) {
+                if ((r & cm_reg) != cm_reg) continue;
+                float2 oR, oI;
+                shfl4(R[r], I[r], oR, oI, xm);
+                float2 yR = R[r], yI = I[r];
+                lane_lin(yR, yI, oR, oI, ar, ai, nai, br, bi, nbi);
+                R[r] = tok ? yR : R[r];
+                I[r] = tok ? yI : I[r];
+            }
+        }
+        return;
+    }
+    if (var == QSV_V_UNI_DIAG) {
+        const float a_r = mine ? m0[6] : m0[0], a_i = mine ? m0[7] : m0[1];
+#pragma unroll
+        for (int r = 0; r < NV; r++) cmul2(R[r], I[r], a_r, a_i);
+        return;
+    }
+    if (var == QSV_V_CTRL_DIAG1 || var == QSV_V_CTRL_DIAG1_SEL) {
+        const bool s = mine && tok;
+        const float d_r = m1[6], d_i = m1[7];
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if ((r & cm_reg) != cm_reg) continue;
+            float2 yR = R[r], yI = I[r];
+            cmul2(yR, yI, d_r, d_i);
+            R[r] = s ? yR : R[r];
+            I[r] = s ? yI : I[r];
+        }
+        return;
+    }
+    if (var == QSV_V_UNI_SWAP || var == QSV_V_CTRL_SWAP || var == QSV_V_CTRL_SWAP_SEL) {
+        const bool uni = var == QSV_V_UNI_SWAP;
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            if (!uni && (r & cm_reg) != cm_reg) continue;
+            float2 oR, oI;
+            shfl4(R[r], I[r], oR, oI, xm);
+            R[r] = (uni || tok) ? oR : R[r];
+            I[r] = (uni || tok) ? oI : I[r];
+        }
+        return;
+    }
+    if (var == QSV_V_SKIP) return;
+    if (var == QSV_V_MUX && op.kind == QSV_K_CTRL && op.cm_c) {
+        // M0 = identity, tile bit 0 among the controls: only the .y halves can be selected
+        if (op.cls1 == QSV_M_XSWAP) {
+#pragma unroll
+            for (int r = 0; r < NV; r++) {
+                if ((r & cm_reg) != cm_reg) continue;
+                const float oR = __shfl_xor_sync(0xffffffffu, R[r].y, xm);
+                const float oI = __shfl_xor_sync(0xffffffffu, I[r].y, xm);
+                R[r].y = tok ? oR : R[r].y;
+                I[r].y = tok ? oI : I[r].y;
+            }
+            return;
+        }
+        if (op.cls1 == QSV_M_DIAG1) {
+            const bool s = mine && tok;
+#pragma unroll
+            for (int r = 0; r < NV; r++) {
+                if ((r & cm_reg) != cm_reg) continue;
+                float yr, yi;
+                diag_own(yr, yi, m1[6], m1[7], R[r].y, I[r].y);
+                R[r].y = s ? yr : R[r].y;
+                I[r].y = s ? yi : I[r].y;
+            }
+            return;
+        }
+        if (op.cls1 == QSV_M_DENSE || op.cls1 == QSV_M_DIAG) {
+            const float a_r = mine ? m1[6] : m1[0], a_i = mine ? m1[7] : m1[1];
+            const float b_r = mine ? m1[4] : m1[2], b_i = mine ? m1[5] : m1[3];
+#pragma unroll
+            for (int r = 0; r < NV; r++) {
+                if ((r & cm_reg) != cm_reg) continue;
+                const float oR = __shfl_xor_sync(0xffffffffu, R[r].y, xm);
+                const float oI = __shfl_xor_sync(0xffffffffu, I[r].y, xm);
+                float yr, yi;
+                lin_own(yr, yi, a_r, a_i, b_r, b_i, R[r].y, I[r].y, oR, oI);
+                R[r].y = tok ? yr : R[r].y;
+                I[r].y = tok ? yi : I[r].y;
+            }
+            return;
+        }
+    }
+    lane_op<NV>(R, I, op, m0, m1, tok, lanebit, lane);
+}
+
 template <int NV, int RB>
 __device__ __forceinline__ void apply_op(const QsvOp &op, float2 (&R)[NV], float2 (&I)[NV], uint32_t tb, int lane) {
     if (op.variant == QSV_V_SKIP) return;
@@ -202,11 +399,11 @@ __device__ __forceinline__ void apply_op(const QsvOp &op, float2 (&R)[NV], float
     const bool thread_ok = (tb & cm_thr) == cm_thr;
     const int slot = op.slot;
     if (slot >= QSV_SLOT_LANE0) {
-        lane_op<NV>(R, I, op, m0, m1, thread_ok, slot - QSV_SLOT_LANE0, lane);
+        lane_op_fast<NV>(R, I, op, m0, m1, thread_ok, slot - QSV_SLOT_LANE0, lane);
         return;
     }
     switch (slot) {
-        case QSV_SLOT_COMP: comp_op<NV>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_SLOT_COMP: comp_op_fast<NV>(R, I, op, m0, m1, thread_ok); break;
         case QSV_SLOT_REG0 + 0: reg_op<NV, 0>(R, I, op, m0, m1, thread_ok); break;
         case QSV_SLOT_REG0 + 1: if constexpr (RB > 1) reg_op<NV, (RB > 1 ? 1 : 0)>(R, I, op, m0, m1, thread_ok); break;
         case QSV_SLOT_REG0 + 2: if constexpr (RB > 2) reg_op<NV, (RB > 2 ? 2 : 0)>(R, I, op, m0, m1, thread_ok); break;
