@@ -48,6 +48,10 @@ extern "C" {
 #define QSV_ERR_SCRATCH (-6)       /* caller-provided scratch smaller than required */
 
 #define QSV_C64 0                  /* complex64 amplitudes (QSV2, fp32 matrices) */
+#define QSV_C128 1                 /* complex128 amplitudes (QSV2 with FP64 matrices, header word 4 = 1;
+                                      an extension with no reference counterpart: the FPGA engine is
+                                      complex64 only). Accepted by run_segment, remap, zero_state,
+                                      reduce_f64, chunk_probs_f64 and sample_f64. */
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 QSV_API int qsv_version(void);
@@ -58,8 +62,10 @@ QSV_API const char *qsv_last_error(void);
 /* Execute one QSV2 segment (every pass, in order) on the device state in place.
  * Replaces sv_engine (kernels/sv/sv_engine.cpp:302); `seg` is the host copy of the words the reference
  * runtime uploads behind each slice (host/sv/runtime.py:218-225). The segment's L must equal n.
- * Consecutive passes are merged into sweeps whose qubit window fits the engine's 13-qubit tile; the
- * result equals pass-by-pass execution value for value. n in [10, 34]. */
+ * Consecutive passes are merged into sweeps whose qubit window fits the engine's 13-qubit tile (12 for
+ * QSV_C128); the result equals pass-by-pass execution value for value. n in [10, 34]. dtype QSV_C128
+ * needs a segment with FP64 matrices (header word 4 = 1); a segment of the other element type is
+ * rejected with QSV_ERR_BAD_STREAM. */
 QSV_API int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int dtype, void *stream);
 
 /* Qubit permutation, out of place: dst[y] = src[x] with bit j of y = bit perm[j] of x

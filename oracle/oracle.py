@@ -40,7 +40,10 @@ def lib():
         L.qsv_oracle_apply_dense_f64.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int]
         L.qsv_oracle_metrics.argtypes = [P, P, I64, P]
         L.qsv_oracle_reduce_f64.argtypes = [P, ctypes.c_int, P, P]
-        for f in ("run_segment", "check_segment", "remap", "apply_dense_f64", "metrics", "reduce_f64"):
+        L.qsv_oracle_run_segment_c128.argtypes = [P, ctypes.c_int, P, I64, ctypes.c_int]
+        L.qsv_oracle_remap_c128.argtypes = [P, P, ctypes.c_int, P, ctypes.c_int]
+        for f in ("run_segment", "check_segment", "remap", "apply_dense_f64", "metrics", "reduce_f64",
+                  "run_segment_c128", "remap_c128"):
             getattr(L, "qsv_oracle_" + f).restype = I32
         _lib = L
     return _lib
@@ -55,11 +58,13 @@ def _ptr(a):
 
 
 def run_segment(state, seg, nthreads=None):
-    """Execute one QSV2 segment in place on a complex64 numpy state (single slice, L = n)."""
-    assert state.dtype == np.complex64 and state.flags.c_contiguous
+    """Execute one QSV2 segment in place on a numpy state (single slice, L = n): complex64 with a
+    reference-format segment, complex128 with an FP64-matrix segment (header word 4 = 1)."""
+    assert state.dtype in (np.complex64, np.complex128) and state.flags.c_contiguous
     seg = np.ascontiguousarray(seg, dtype=np.int32)
     n = state.size.bit_length() - 1
-    rc = lib().qsv_oracle_run_segment(_ptr(state), n, _ptr(seg), seg.size, nthreads or threads())
+    run = lib().qsv_oracle_run_segment_c128 if state.dtype == np.complex128 else lib().qsv_oracle_run_segment
+    rc = run(_ptr(state), n, _ptr(seg), seg.size, nthreads or threads())
     if rc != 0:
         raise ValueError(f"oracle rejected segment (code {rc})")
     return state
@@ -69,7 +74,8 @@ def remap(state, perm, nthreads=None):
     n = state.size.bit_length() - 1
     perm = np.ascontiguousarray(perm, dtype=np.int32)
     out = np.empty_like(state)
-    rc = lib().qsv_oracle_remap(_ptr(state), _ptr(out), n, _ptr(perm), nthreads or threads())
+    f = lib().qsv_oracle_remap_c128 if state.dtype == np.complex128 else lib().qsv_oracle_remap
+    rc = f(_ptr(state), _ptr(out), n, _ptr(perm), nthreads or threads())
     if rc != 0:
         raise ValueError(f"bad permutation (code {rc})")
     return out
@@ -79,10 +85,10 @@ def unpermute(state, final_map):
     return remap(state, [final_map[q] for q in range(len(final_map))])
 
 
-def run_program(prog, n, final_map, state=None):
+def run_program(prog, n, final_map, state=None, dtype=np.complex64):
     """Whole program from |0...0> with the C engine; returns the logical-order state."""
     if state is None:
-        state = np.zeros(1 << n, dtype=np.complex64)
+        state = np.zeros(1 << n, dtype=dtype)
         state[0] = 1
     for kind, payload in prog:
         if kind == "segment":

@@ -19,7 +19,8 @@
  *   y1.re = fma(m11.re, x1.re, fma(-m11.im, x1.im, fma(m10.re, x0.re, -(m10.im * x0.im))))
  *   y1.im = fma(m11.re, x1.im, fma( m11.im, x1.re, fma(m10.re, x0.im,   m10.im * x0.re)))
  * Also here: an FP64 dense gate-by-gate simulator (the "Qiskit-style statevector" oracle) and FP64
- * reductions used to check the device reductions.
+ * reductions used to check the device reductions, and the complex128 engine (streams with header word
+ * 4 = 1 carry FP64 matrices, 40-word op records; same addressing, the same chain in double precision).
  *
  * Build: gcc -O2 -fPIC -shared -fopenmp -ffp-contract=off (see oracle/Makefile).
  */
@@ -35,6 +36,7 @@
 #define HDR_WORDS 8
 #define PASS_WORDS 8
 #define OP_WORDS 24
+#define OP_WORDS_C128 40
 
 typedef struct { float re, im; } c64;
 
@@ -50,9 +52,12 @@ static inline void pair_update(const float *m, c64 *a, c64 *b) {
     a->re = y0r; a->im = y0i; b->re = y1r; b->im = y1i;
 }
 
-/* Validates a segment; returns number of passes or a negative code. */
-int qsv_oracle_check_segment(const int32_t *seg, int64_t nwords, int n) {
+/* Validates a segment of element type dtype (0 = complex64, 1 = complex128); returns the number of
+ * passes or a negative code. */
+static int check_segment_dt(const int32_t *seg, int64_t nwords, int n, int dtype) {
+    const int opw = dtype ? OP_WORDS_C128 : OP_WORDS;
     if (nwords < HDR_WORDS || seg[0] != QSV_MAGIC) return -1;
+    if (seg[4] != dtype) return -9;
     const int L = seg[1], np = seg[2], k = seg[3];
     if (L != n || k < 1 || k > L || np < 0) return -2;
     int64_t pos = HDR_WORDS;
@@ -67,17 +72,22 @@ int qsv_oracle_check_segment(const int32_t *seg, int64_t nwords, int n) {
         }
         pos += PASS_WORDS;
         for (int o = 0; o < nops; o++) {
-            if (pos + OP_WORDS > nwords) return -3;
+            if (pos + opw > nwords) return -3;
             if (seg[pos] != 1) return -6;
             const int t = seg[pos + 1];
             const uint32_t cm = (uint32_t)seg[pos + 2];
             if (t < 0 || t >= k) return -7;
             if (k < 32 && (cm >> k)) return -7;
-            pos += OP_WORDS;
+            pos += opw;
         }
     }
     if (pos != nwords) return -8;
     return np;
+}
+
+/* Validates a complex64 segment; returns number of passes or a negative code. */
+int qsv_oracle_check_segment(const int32_t *seg, int64_t nwords, int n) {
+    return check_segment_dt(seg, nwords, n, 0);
 }
 
 /* Execute one QSV2 segment on a complex64 state of 2^n amplitudes in place (model.py:59-71, P = 1). */
@@ -158,11 +168,95 @@ int qsv_oracle_remap(const float *src, float *dst, int n, const int32_t *perm, i
     return 0;
 }
 
-/* ------------------------------------------------------------------ FP64 dense oracle */
 typedef struct { double re, im; } c128;
+
+/* ------------------------------------------------------------------ complex128 engine */
+
+static inline double d_of(const int32_t *w) { double d; memcpy(&d, w, 8); return d; }
+
+/* the canonical chain in double precision */
+static inline void pair_update_d(const double *m, c128 *a, c128 *b) {
+    const double x0r = a->re, x0i = a->im, x1r = b->re, x1i = b->im;
+    const double y0r = fma(m[0], x0r, fma(-m[1], x0i, fma(m[2], x1r, -(m[3] * x1i))));
+    const double y0i = fma(m[0], x0i, fma(m[1], x0r, fma(m[2], x1i, m[3] * x1r)));
+    const double y1r = fma(m[6], x1r, fma(-m[7], x1i, fma(m[4], x0r, -(m[5] * x0i))));
+    const double y1i = fma(m[6], x1i, fma(m[7], x1r, fma(m[4], x0i, m[5] * x0r)));
+    a->re = y0r; a->im = y0i; b->re = y1r; b->im = y1i;
+}
+
+/* Execute one complex128 segment (header word 4 = 1) on a complex128 state in place. */
+int qsv_oracle_run_segment_c128(double *state, int n, const int32_t *seg, int64_t nwords, int nthreads) {
+    const int np = check_segment_dt(seg, nwords, n, 1);
+    if (np < 0) return np;
+    const int L = seg[1], k = seg[3];
+    c128 *st = (c128 *)state;
+    int64_t pos = HDR_WORDS;
+    for (int p = 0; p < np; p++) {
+        const int m = seg[pos], nops = seg[pos + 3];
+        const int h[4] = {seg[pos + 1], seg[pos + 2], seg[pos + 4], seg[pos + 5]};
+        const int32_t *ops = seg + pos + PASS_WORDS;
+        pos += PASS_WORDS + (int64_t)nops * OP_WORDS_C128;
+        const int low = k - m;
+        int free_bits[64], nfree = 0;
+        for (int b = 0; b < L; b++) {
+            int used = b < low;
+            for (int i = 0; i < m; i++) used |= (b == h[i]);
+            if (!used) free_bits[nfree++] = b;
+        }
+        const int64_t ntiles = (int64_t)1 << nfree, tsize = (int64_t)1 << k;
+        int64_t *off = (int64_t *)malloc(sizeof(int64_t) * tsize);
+        for (int64_t j = 0; j < tsize; j++) {
+            int64_t o = j & (((int64_t)1 << low) - 1);
+            for (int i = 0; i < m; i++) o |= ((j >> (low + i)) & 1) << h[i];
+            off[j] = o;
+        }
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+        {
+            c128 *T = (c128 *)malloc(sizeof(c128) * tsize);
+#pragma omp for schedule(static)
+            for (int64_t t = 0; t < ntiles; t++) {
+                int64_t base = 0;
+                for (int i = 0; i < nfree; i++) base |= ((t >> i) & 1) << free_bits[i];
+                for (int64_t j = 0; j < tsize; j++) T[j] = st[base | off[j]];
+                for (int o = 0; o < nops; o++) {
+                    const int32_t *rec = ops + (int64_t)o * OP_WORDS_C128;
+                    const int tq = rec[1];
+                    const int64_t cm = (uint32_t)rec[2];
+                    double M0[8], M1[8];
+                    for (int e = 0; e < 8; e++) { M0[e] = d_of(rec + 8 + 2 * e); M1[e] = d_of(rec + 24 + 2 * e); }
+                    const int64_t bit = (int64_t)1 << tq;
+                    for (int64_t i0 = 0; i0 < tsize; i0++) {
+                        if (i0 & bit) continue;
+                        const int sel = cm != 0 && (i0 & cm) == cm;
+                        pair_update_d(sel ? M1 : M0, &T[i0], &T[i0 | bit]);
+                    }
+                }
+                for (int64_t j = 0; j < tsize; j++) st[base | off[j]] = T[j];
+            }
+            free(T);
+        }
+        free(off);
+    }
+    return 0;
+}
+
+/* complex128 remap: dst[y] = src[x], bit j of y = bit perm[j] of x. */
+int qsv_oracle_remap_c128(const double *src, double *dst, int n, const int32_t *perm, int nthreads) {
+    const int64_t N = (int64_t)1 << n;
+    const c128 *s = (const c128 *)src;
+    c128 *d = (c128 *)dst;
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static)
+    for (int64_t y = 0; y < N; y++) {
+        int64_t x = 0;
+        for (int j = 0; j < n; j++) x |= ((y >> j) & 1) << perm[j];
+        d[y] = s[x];
+    }
+    return 0;
+}
 
 /* Apply a dense 2^nq x 2^nq complex128 matrix (row-major, Qiskit little-endian over `qubits`) to the
  * complex128 state of 2^n amplitudes in place. */
+/* ------------------------------------------------------------------ FP64 dense oracle */
 int qsv_oracle_apply_dense_f64(double *state, int n, const int32_t *qubits, int nq, const double *mat,
                                int nthreads) {
     if (nq < 1 || nq > 12 || nq > n) return -1;

@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 from scipy.linalg import cossin
 
-from .isa import MAGIC, OP_MUX2, MAX_OPS_PER_PASS, MAX_HIGH
+from .isa import MAGIC, OP_MUX2, MAX_OPS_PER_PASS, MAX_HIGH, DTYPE_C64, DTYPE_C128
 from .gates import I2, X, Z, gate_matrix, mc_matrix, phase
 from .circuit import normalize
 
@@ -287,10 +287,14 @@ def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=
     return steps, l2p
 
 
-def encode_segment(passes, L, k, M=MAX_HIGH):
-    """QSV2 words of one segment (compiler.py:263-285). Matrices are rounded to complex64 here: this
-    is the single FP64 -> FP32 rounding point of the program."""
-    words = [MAGIC, L, len(passes), k, 0, 0, 0, 0]
+def encode_segment(passes, L, k, M=MAX_HIGH, dtype="c64"):
+    """QSV2 words of one segment (compiler.py:263-285). For dtype "c64" (the reference's format) the
+    matrices are rounded to complex64 here: this is the single FP64 -> FP32 rounding point of the program.
+    For "c128" (complex128 states; header word 4 = DTYPE_C128) the FP64 matrices are stored as they are."""
+    c128 = dtype == "c128"
+    if dtype not in ("c64", "c128"):
+        raise ValueError(f"dtype must be 'c64' or 'c128', not {dtype!r}")
+    words = [MAGIC, L, len(passes), k, DTYPE_C128 if c128 else DTYPE_C64, 0, 0, 0]
     for p in passes:
         qubits = set(q for _, ph in p for q in ph)
         m, hi = pass_window(qubits, k, M)
@@ -304,11 +308,16 @@ def encode_segment(passes, L, k, M=MAX_HIGH):
         for j, (op, ph) in enumerate(p):
             mats[j, 0] = np.asarray(op.M0, dtype=complex).reshape(-1)
             mats[j, 1] = np.asarray(op.M1, dtype=complex).reshape(-1)
-        c64 = mats.astype(np.complex64)
-        fl = np.empty((len(p), 16), dtype=np.float32)
-        fl[:, 0:8:2], fl[:, 1:8:2] = c64[:, 0].real, c64[:, 0].imag
-        fl[:, 8:16:2], fl[:, 9:16:2] = c64[:, 1].real, c64[:, 1].imag
-        fbits = fl.view(np.int32)
+        if c128:
+            fl = np.empty((len(p), 16), dtype=np.float64)
+            fl[:, 0:8:2], fl[:, 1:8:2] = mats[:, 0].real, mats[:, 0].imag
+            fl[:, 8:16:2], fl[:, 9:16:2] = mats[:, 1].real, mats[:, 1].imag
+        else:
+            c64 = mats.astype(np.complex64)
+            fl = np.empty((len(p), 16), dtype=np.float32)
+            fl[:, 0:8:2], fl[:, 1:8:2] = c64[:, 0].real, c64[:, 0].imag
+            fl[:, 8:16:2], fl[:, 9:16:2] = c64[:, 1].real, c64[:, 1].imag
+        fbits = np.ascontiguousarray(fl).view(np.int32)
         for j, (op, ph) in enumerate(p):
             tq = [tile_of[q] for q in ph]
             cmask = 0
@@ -320,10 +329,16 @@ def encode_segment(passes, L, k, M=MAX_HIGH):
     return (arr & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
 
 
+def segment_dtype(seg):
+    """"c64" or "c128" from a segment's header word 4."""
+    return "c128" if int(np.asarray(seg)[4]) == DTYPE_C128 else "c64"
+
+
 def compile_circuit(qc, L, k, fuse_1q=True, tiling=True, remap_policy="lru", initial_map=None,
-                    max_high=MAX_HIGH):
+                    max_high=MAX_HIGH, dtype="c64"):
     """Full pipeline (compiler.py:288-314). Returns (prog, final_map, stats); final_map[l] is the
-    physical position of logical qubit l after the program."""
+    physical position of logical qubit l after the program. dtype "c128" emits segments with FP64
+    matrices for complex128 states (an extension of the stream, see isa.py)."""
     k = min(k, L)
     max_high = max(0, min(max_high, k - 3))      # sub-blocks of at least 2^3 amplitudes
     stats = Stats()
@@ -338,7 +353,7 @@ def compile_circuit(qc, L, k, fuse_1q=True, tiling=True, remap_policy="lru", ini
         prog.append(("remap", perm))
     for kind, payload in steps:
         if kind == "segment":
-            prog.append(("segment", encode_segment(payload, L, k, max_high)))
+            prog.append(("segment", encode_segment(payload, L, k, max_high, dtype)))
             stats.n_segments += 1
             stats.n_passes += len(payload)
         else:

@@ -30,10 +30,12 @@ struct RemapParams {
     uint8_t ypos[REMAP_TB];         // destination position of tile source bit ubits[i]
 };
 
+// A = float2 (complex64) or double2 (complex128)
+template <class A>
 __global__ void __launch_bounds__(REMAP_THREADS)
-    remap_kernel(const float2 *__restrict__ src, float2 *__restrict__ dst, const __grid_constant__ RemapParams P) {
+    remap_kernel(const A *__restrict__ src, A *__restrict__ dst, const __grid_constant__ RemapParams P) {
     constexpr int TS = 1 << REMAP_TB;
-    __shared__ float2 tile[TS];
+    __shared__ A tile[TS];
     __shared__ uint64_t rd_off[TS];
     __shared__ uint64_t wr_off[TS];
     __shared__ uint16_t wr_pos[TS];
@@ -83,14 +85,16 @@ __global__ void __launch_bounds__(REMAP_THREADS)
 
 // ---------------------------------------------------------------- |0...0>
 __global__ void set_amp0_kernel(float2 *state) { state[0] = make_float2(1.0f, 0.0f); }
+__global__ void set_amp0_kernel_d(double2 *state) { state[0] = make_double2(1.0, 0.0); }
 
 // ---------------------------------------------------------------- FP64 reductions
 // Block b covers amplitudes [b << B, (b+1) << B). Thread t visits i = (b << B) + t + 256 * it. The
 // per-block result is 1 + B doubles: the block total and, for each bit q < B of the index, the sum of
 // |a_i|^2 over the block's i with bit q set. Fixed summation order (deterministic).
 #define RED_THREADS 256
+template <class A>
 __global__ void __launch_bounds__(RED_THREADS)
-    reduce_block_kernel(const float2 *__restrict__ state, int B, double *__restrict__ partials) {
+    reduce_block_kernel(const A *__restrict__ state, int B, double *__restrict__ partials) {
     __shared__ double s_tot[RED_THREADS];
     __shared__ double s_bits[RED_THREADS][17];
     const int t = threadIdx.x;
@@ -110,7 +114,7 @@ __global__ void __launch_bounds__(RED_THREADS)
         for (int k = 0; k < 16; k++) {
             u[k] = 0.0;
             if (k < gk) {
-                const float2 a = state[base + t + ((int64_t)((g << 4) | k) << 8)];
+                const A a = state[base + t + ((int64_t)((g << 4) | k) << 8)];
                 u[k] = (double)a.x * a.x + (double)a.y * a.y;
             }
         }
@@ -170,14 +174,15 @@ __global__ void reduce_final_kernel(const double *__restrict__ partials, int nbl
 }
 
 // chunk probabilities: one block per chunk of 2^cb amplitudes
+template <class A>
 __global__ void __launch_bounds__(RED_THREADS)
-    chunk_probs_kernel(const float2 *__restrict__ state, int cb, double *__restrict__ out) {
+    chunk_probs_kernel(const A *__restrict__ state, int cb, double *__restrict__ out) {
     __shared__ double s[RED_THREADS];
     const int64_t base = (int64_t)blockIdx.x << cb;
     const int len = 1 << cb;
     double acc = 0.0;
     for (int i = threadIdx.x; i < len; i += RED_THREADS) {
-        const float2 a = state[base + i];
+        const A a = state[base + i];
         acc += (double)a.x * a.x + (double)a.y * a.y;
     }
     s[threadIdx.x] = acc;
@@ -217,7 +222,8 @@ __global__ void scan_kernel(double *__restrict__ v, int64_t nc) {
 
 // one thread per shot: chunk by binary search on the FP64 chunk cdf, then a linear FP64 scan inside
 // the chunk (first index whose running sum exceeds the remainder, clipped to the chunk)
-__global__ void sample_kernel(const float2 *__restrict__ state, int cb, const double *__restrict__ cdf, int64_t nc,
+template <class A>
+__global__ void sample_kernel(const A *__restrict__ state, int cb, const double *__restrict__ cdf, int64_t nc,
                               const double *__restrict__ uni, int shots, int64_t *__restrict__ out) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= shots) return;
@@ -232,11 +238,11 @@ __global__ void sample_kernel(const float2 *__restrict__ state, int cb, const do
     int64_t c = lo < nc ? lo : nc - 1;
     const double rem = x - (c > 0 ? cdf[c - 1] : 0.0);
     const int len = 1 << cb;
-    const float2 *p = state + (c << cb);
+    const A *p = state + (c << cb);
     double run = 0.0;
     int j = 0;
     for (; j < len; j++) {
-        const float2 a = p[j];
+        const A a = p[j];
         run += (double)a.x * a.x + (double)a.y * a.y;
         if (run > rem) break;
     }
@@ -247,7 +253,9 @@ __global__ void sample_kernel(const float2 *__restrict__ state, int cb, const do
 }  // namespace dev
 
 // ---------------------------------------------------------------- host launchers
-cudaError_t launch_remap(const float2 *src, float2 *dst, int n, const int32_t *perm, int nsm, cudaStream_t stream) {
+// dtype: 0 = complex64 (float2 amplitudes), 1 = complex128 (double2)
+cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, int nsm,
+                         cudaStream_t stream) {
     dev::RemapParams P;
     memset(&P, 0, sizeof(P));
     P.n = n;
@@ -276,12 +284,16 @@ cudaError_t launch_remap(const float2 *src, float2 *dst, int n, const int32_t *p
     const int64_t ntiles = 1ll << nf;
     int64_t grid = (int64_t)nsm * 8;
     if (grid > ntiles) grid = ntiles;
-    dev::remap_kernel<<<(unsigned)grid, REMAP_THREADS, 0, stream>>>(src, dst, P);
+    if (dtype)
+        dev::remap_kernel<double2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const double2 *)src, (double2 *)dst, P);
+    else
+        dev::remap_kernel<float2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const float2 *)src, (float2 *)dst, P);
     return cudaGetLastError();
 }
 
-cudaError_t launch_set_amp0(float2 *state, cudaStream_t stream) {
-    dev::set_amp0_kernel<<<1, 1, 0, stream>>>(state);
+cudaError_t launch_set_amp0(void *state, int dtype, cudaStream_t stream) {
+    if (dtype) dev::set_amp0_kernel_d<<<1, 1, 0, stream>>>((double2 *)state);
+    else dev::set_amp0_kernel<<<1, 1, 0, stream>>>((float2 *)state);
     return cudaGetLastError();
 }
 
@@ -300,11 +312,12 @@ size_t reduce_scratch_bytes(int n, int chunk_bits) {
     return red > smp ? red : smp;
 }
 
-cudaError_t launch_reduce(const float2 *state, int n, double *out, void *scratch, cudaStream_t stream) {
+cudaError_t launch_reduce(const void *state, int n, int dtype, double *out, void *scratch, cudaStream_t stream) {
     const int B = reduce_bits(n);
     const int nblocks = 1 << (n - B);
     double *partials = (double *)scratch;
-    dev::reduce_block_kernel<<<nblocks, RED_THREADS, 0, stream>>>(state, B, partials);
+    if (dtype) dev::reduce_block_kernel<double2><<<nblocks, RED_THREADS, 0, stream>>>((const double2 *)state, B, partials);
+    else dev::reduce_block_kernel<float2><<<nblocks, RED_THREADS, 0, stream>>>((const float2 *)state, B, partials);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dev::reduce_final_kernel<<<1, 64, 0, stream>>>(partials, nblocks, B, n, out);
@@ -340,7 +353,7 @@ static cudaError_t noalloc_scratch_ptr(double **out) {
     return cudaSuccess;
 }
 
-cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need) {
+cudaError_t launch_reduce_noalloc(const void *state, int n, double *out, cudaStream_t stream, size_t *need) {
     const int B = reduce_bits(n);
     const size_t doubles = ((size_t)1 << (n - B)) * (B + 1);
     *need = doubles * sizeof(double);
@@ -348,25 +361,35 @@ cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaS
     double *scratch = nullptr;
     cudaError_t e = noalloc_scratch_ptr(&scratch);
     if (e != cudaSuccess) return e;
-    return launch_reduce(state, n, out, scratch, stream);
+    return launch_reduce(state, n, 0, out, scratch, stream);
 }
 
-cudaError_t launch_chunk_probs(const float2 *state, int n, int cb, double *out, cudaStream_t stream) {
-    dev::chunk_probs_kernel<<<(unsigned)(1ll << (n - cb)), RED_THREADS, 0, stream>>>(state, cb, out);
+cudaError_t launch_chunk_probs(const void *state, int n, int dtype, int cb, double *out, cudaStream_t stream) {
+    const unsigned nc = (unsigned)(1ll << (n - cb));
+    if (dtype) dev::chunk_probs_kernel<double2><<<nc, RED_THREADS, 0, stream>>>((const double2 *)state, cb, out);
+    else dev::chunk_probs_kernel<float2><<<nc, RED_THREADS, 0, stream>>>((const float2 *)state, cb, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni, int shots, int64_t *out,
+cudaError_t launch_sample(const void *state, int n, int dtype, int cb, const double *uni, int shots, int64_t *out,
                           void *scratch, cudaStream_t stream) {
     double *cdf = (double *)scratch;
     const int64_t nc = 1ll << (n - cb);
-    dev::chunk_probs_kernel<<<(unsigned)nc, RED_THREADS, 0, stream>>>(state, cb, cdf);
+    cudaError_t e0 = launch_chunk_probs(state, n, dtype, cb, cdf, stream);
+    if (e0 != cudaSuccess) return e0;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dev::scan_kernel<<<1, 1024, 0, stream>>>(cdf, nc);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (shots > 0) dev::sample_kernel<<<(shots + 127) / 128, 128, 0, stream>>>(state, cb, cdf, nc, uni, shots, out);
+    if (shots > 0) {
+        if (dtype)
+            dev::sample_kernel<double2><<<(shots + 127) / 128, 128, 0, stream>>>((const double2 *)state, cb, cdf, nc, uni,
+                                                                                 shots, out);
+        else
+            dev::sample_kernel<float2><<<(shots + 127) / 128, 128, 0, stream>>>((const float2 *)state, cb, cdf, nc, uni,
+                                                                                shots, out);
+    }
     return cudaGetLastError();
 }
 

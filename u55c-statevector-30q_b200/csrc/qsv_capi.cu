@@ -12,11 +12,13 @@
 
 namespace qsv {
 cudaError_t launch_sweep(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream);
-cudaError_t launch_remap(const float2 *src, float2 *dst, int n, const int32_t *perm, int nsm, cudaStream_t stream);
-cudaError_t launch_set_amp0(float2 *state, cudaStream_t stream);
-cudaError_t launch_reduce(const float2 *state, int n, double *out, void *scratch, cudaStream_t stream);
-cudaError_t launch_chunk_probs(const float2 *state, int n, int cb, double *out, cudaStream_t stream);
-cudaError_t launch_sample(const float2 *state, int n, int cb, const double *uni, int shots, int64_t *out,
+cudaError_t launch_sweep_c128(double2 *state, const QsvSweepD &sw, int nsm, cudaStream_t stream);
+cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, int nsm,
+                         cudaStream_t stream);
+cudaError_t launch_set_amp0(void *state, int dtype, cudaStream_t stream);
+cudaError_t launch_reduce(const void *state, int n, int dtype, double *out, void *scratch, cudaStream_t stream);
+cudaError_t launch_chunk_probs(const void *state, int n, int dtype, int cb, double *out, cudaStream_t stream);
+cudaError_t launch_sample(const void *state, int n, int dtype, int cb, const double *uni, int shots, int64_t *out,
                           void *scratch, cudaStream_t stream);
 size_t reduce_scratch_bytes(int n, int chunk_bits);
 cudaError_t take_device_status(int *out);
@@ -27,7 +29,7 @@ int batch_add(Batch *b, void *state, int n, int nseg, const int32_t *const *segs
 size_t batch_workspace_bytes(Batch *b);
 cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
 cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
-cudaError_t launch_reduce_noalloc(const float2 *state, int n, double *out, cudaStream_t stream, size_t *need);
+cudaError_t launch_reduce_noalloc(const void *state, int n, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
 int jit_set_mode(int mode);
 int jit_prepare(const std::vector<QsvSweep> &sweeps);
@@ -44,6 +46,8 @@ static int g_lo_merge = 4;             // merged sweeps keep sub-blocks of >= 2^
 
 static const int QSV_CHUNK_BITS = 12;  // sampler chunk: 2^12 amplitudes (host/sv/runtime.py:47 chunk_bits=12)
 static int chunk_bits_for(int n) { return n < QSV_CHUNK_BITS ? n : QSV_CHUNK_BITS; }
+static bool dtype_ok(int dtype) { return dtype == QSV_C64 || dtype == QSV_C128; }
+static size_t amp_bytes(int dtype) { return dtype == QSV_C128 ? 16 : 8; }
 static const int QSV_N_MIN = 10;
 static const int QSV_N_MAX = 34;
 
@@ -96,24 +100,37 @@ int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, siz
     if (rc) return fail(rc, err);
     std::vector<QsvSweep> sweeps;
     const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
-    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
     if (rc) return fail(rc, err);
     return qsv::serialize(sweeps, out, cap);
 }
 
 int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int dtype, void *stream) {
     if (!state) return fail(QSV_ERR_INVALID_ARG, "state is null");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 segments are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     std::vector<qsv::PhysPass> passes;
     std::string err;
-    int rc = qsv::decode_segment(seg, nwords, n, passes, err);
-    if (rc) return fail(rc, err);
-    std::vector<QsvSweep> sweeps;
-    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
-    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    int rc = qsv::decode_segment(seg, nwords, n, passes, err, dtype);
     if (rc) return fail(rc, err);
     const int nsm = sm_count();
+    if (dtype == QSV_C128) {
+        std::vector<QsvSweepD> sweeps;
+        const int kw = n < 12 ? n : 12;
+        rc = qsv::build_sweeps<QsvOpD>(passes, n, kw, g_lo_merge, sweeps, err);
+        if (rc) return fail(rc, err);
+        std::lock_guard<std::mutex> lk(g_launch_mu);
+        for (const QsvSweepD &sw : sweeps) {
+            cudaError_t e = qsv::launch_sweep_c128((double2 *)state, sw, nsm, (cudaStream_t)stream);
+            if (e != cudaSuccess) return cuda_fail(e, "complex128 sweep launch");
+            t_launches++;
+        }
+        return QSV_OK;
+    }
+    std::vector<QsvSweep> sweeps;
+    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+    rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
+    if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lk(g_launch_mu);
     for (const QsvSweep &sw : sweeps) {
         cudaError_t e = cudaSuccess;
@@ -142,7 +159,7 @@ int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n) {
     if (rc) return fail(rc, err);
     std::vector<QsvSweep> sweeps;
     const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
-    rc = qsv::build_sweeps(passes, n, kw, g_lo_merge, sweeps, err);
+    rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
     if (rc) return fail(rc, err);
     const int ready = qsv::jit_prepare(sweeps);
     const std::string log = qsv::jit_last_log();
@@ -162,7 +179,7 @@ int qsv_jit_info(long long *out, int cap) {
 
 int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, void *stream) {
     if (!src || !dst || !perm) return fail(QSV_ERR_INVALID_ARG, "null pointer");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     if (src == dst) return fail(QSV_ERR_INVALID_ARG, "remap is out of place: src == dst");
     bool seen[64] = {false};
@@ -170,7 +187,7 @@ int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype,
         if (perm[j] < 0 || perm[j] >= n || seen[perm[j]]) return fail(QSV_ERR_INVALID_ARG, "perm is not a permutation");
         seen[perm[j]] = true;
     }
-    cudaError_t e = qsv::launch_remap((const float2 *)src, (float2 *)dst, n, perm, sm_count(), (cudaStream_t)stream);
+    cudaError_t e = qsv::launch_remap(src, dst, n, perm, dtype, sm_count(), (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "remap launch");
     t_launches++;
     return QSV_OK;
@@ -178,11 +195,11 @@ int qsv_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype,
 
 int qsv_zero_state(void *state, int n, int dtype, void *stream) {
     if (!state) return fail(QSV_ERR_INVALID_ARG, "state is null");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < 1 || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of range");
-    cudaError_t e = cudaMemsetAsync(state, 0, (size_t)8 << n, (cudaStream_t)stream);
+    cudaError_t e = cudaMemsetAsync(state, 0, amp_bytes(dtype) << n, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "memset");
-    e = qsv::launch_set_amp0((float2 *)state, (cudaStream_t)stream);
+    e = qsv::launch_set_amp0(state, dtype, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "init launch");
     t_launches++;
     return QSV_OK;
@@ -196,10 +213,10 @@ size_t qsv_reduce_scratch_bytes(int n) {
 int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *scratch, size_t scratch_bytes,
                    void *stream) {
     if (!state || !out_dev || !scratch) return fail(QSV_ERR_INVALID_ARG, "null pointer");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     if (scratch_bytes < qsv_reduce_scratch_bytes(n)) return fail(QSV_ERR_SCRATCH, "scratch too small");
-    cudaError_t e = qsv::launch_reduce((const float2 *)state, n, out_dev, scratch, (cudaStream_t)stream);
+    cudaError_t e = qsv::launch_reduce(state, n, dtype, out_dev, scratch, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "reduce launch");
     t_launches += 2;
     return QSV_OK;
@@ -211,7 +228,7 @@ int qsv_reduce_f64_noalloc(const void *state, int n, int dtype, double *out_dev,
     if (n < QSV_N_MIN || n > QSV_N_MAX)
         return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34] for the fixed-scratch reduction");
     size_t need = 0;
-    cudaError_t e = qsv::launch_reduce_noalloc((const float2 *)state, n, out_dev, (cudaStream_t)stream, &need);
+    cudaError_t e = qsv::launch_reduce_noalloc(state, n, out_dev, (cudaStream_t)stream, &need);
     if (need > qsv::noalloc_reduce_capacity())
         return fail(QSV_ERR_SCRATCH, "state needs " + std::to_string(need) + " B of block partials, fixed scratch holds " +
                                          std::to_string(qsv::noalloc_reduce_capacity()) + " B");
@@ -222,10 +239,10 @@ int qsv_reduce_f64_noalloc(const void *state, int n, int dtype, double *out_dev,
 
 int qsv_chunk_probs_f64(const void *state, int n, int dtype, int chunk_bits, double *out_dev, void *stream) {
     if (!state || !out_dev) return fail(QSV_ERR_INVALID_ARG, "null pointer");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX || chunk_bits < 0 || chunk_bits > n)
         return fail(QSV_ERR_INVALID_ARG, "n or chunk_bits out of range");
-    cudaError_t e = qsv::launch_chunk_probs((const float2 *)state, n, chunk_bits, out_dev, (cudaStream_t)stream);
+    cudaError_t e = qsv::launch_chunk_probs(state, n, dtype, chunk_bits, out_dev, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "chunk launch");
     t_launches++;
     return QSV_OK;
@@ -234,10 +251,10 @@ int qsv_chunk_probs_f64(const void *state, int n, int dtype, int chunk_bits, dou
 int qsv_sample_f64(const void *state, int n, int dtype, const double *uniforms_dev, int shots, int64_t *out_dev,
                    void *scratch, size_t scratch_bytes, void *stream) {
     if (!state || !scratch || (shots > 0 && (!uniforms_dev || !out_dev))) return fail(QSV_ERR_INVALID_ARG, "null pointer");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX || shots < 0) return fail(QSV_ERR_INVALID_ARG, "n or shots out of range");
     if (scratch_bytes < qsv_reduce_scratch_bytes(n)) return fail(QSV_ERR_SCRATCH, "scratch too small");
-    cudaError_t e = qsv::launch_sample((const float2 *)state, n, chunk_bits_for(n), uniforms_dev, shots, out_dev, scratch,
+    cudaError_t e = qsv::launch_sample(state, n, dtype, chunk_bits_for(n), uniforms_dev, shots, out_dev, scratch,
                                        (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "sample launch");
     t_launches += 3;

@@ -143,6 +143,8 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
     std::ostringstream s;
     s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
       << "namespace qsv {\nnamespace dev {\nstruct JitBody {\n"
+      << "    using Amp = float2;\n"
+      << "    static constexpr int kHalfBits = 1;\n"
       << "    static constexpr bool kSmemOps = false;\n"
       << "    template <int NV, int RB, int WB>\n"
       << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *, int lane, int warp,\n"

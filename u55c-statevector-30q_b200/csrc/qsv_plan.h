@@ -94,6 +94,24 @@ struct QsvOp {
     uint8_t pad[3];
 };
 
+// complex128 op: the same fields with FP64 matrices. In the complex128 layout tile bits 0-2 are lane bits
+// 0-2 (one 16-byte amplitude per slot), so there is no QSV_SLOT_COMP and cm_c is always 0.
+struct QsvOpD {
+    double m0[8];
+    double m1[8];
+    uint32_t cmask;
+    uint32_t cm_thr;
+    uint8_t cm_reg;
+    uint8_t cm_c;
+    uint8_t kind;
+    uint8_t cls;
+    uint8_t cls0, cls1;
+    uint8_t slot;
+    uint8_t tbit;
+    uint8_t variant;
+    uint8_t pad[7];
+};
+
 struct QsvPhase {
     uint8_t reg_bits[QSV_RB_MAX];
     uint8_t lane_bits[2];
@@ -111,7 +129,9 @@ struct QsvPhaseX {
     int32_t op_begin, op_end;
 };
 
-struct QsvSweep {
+template <class OpT>
+struct QsvSweepT {
+    typedef OpT op_type;
     int32_t n;                  // state qubits
     int32_t kw;                 // window size (tile = 2^kw amplitudes)
     int32_t lo;                 // contiguous low bits of the window
@@ -125,5 +145,7 @@ struct QsvSweep {
     int32_t nphases;
     int32_t nops;
     QsvPhase phases[QSV_MAX_PHASES];
-    QsvOp ops[QSV_MAX_SWEEP_OPS];
+    OpT ops[QSV_MAX_SWEEP_OPS];
 };
+typedef QsvSweepT<QsvOp> QsvSweep;      // complex64 state, fp32 matrices
+typedef QsvSweepT<QsvOpD> QsvSweepD;    // complex128 state, fp64 matrices

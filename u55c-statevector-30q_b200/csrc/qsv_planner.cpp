@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 namespace qsv {
 
@@ -17,10 +18,24 @@ static inline float f_of(int32_t w) {
     return f;
 }
 
-int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPass> &out, std::string &err) {
+static inline double d_of(const int32_t *w) {
+    double d;
+    std::memcpy(&d, w, 8);
+    return d;
+}
+
+int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPass> &out, std::string &err,
+                   int dtype) {
     out.clear();
     if (!seg || nwords < QSV2_HDR_WORDS) { err = "segment shorter than its header"; return QSV_ERR_BAD_STREAM; }
     if ((uint32_t)seg[0] != QSV2_MAGIC) { err = "bad QSV2 magic"; return QSV_ERR_BAD_STREAM; }
+    if (seg[4] != dtype) {
+        err = seg[4] == 1 ? "segment carries FP64 matrices (complex128) but the state is complex64"
+              : seg[4] == 0 ? "segment carries FP32 matrices (complex64) but the state is complex128"
+                            : "unknown element type in header word 4";
+        return QSV_ERR_BAD_STREAM;
+    }
+    const size_t opw = dtype ? QSV2_OP_WORDS_C128 : QSV2_OP_WORDS;
     const int L = seg[1], npass = seg[2], k = seg[3];
     if (L != n) { err = "segment L (" + std::to_string(L) + ") != state qubits (" + std::to_string(n) + ")"; return QSV_ERR_BAD_STREAM; }
     if (k < 1 || k > L || npass < 0) { err = "bad segment header (k, n_passes)"; return QSV_ERR_BAD_STREAM; }
@@ -38,7 +53,7 @@ int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPas
         pos += QSV2_PASS_WORDS;
         PhysPass pp;
         for (int o = 0; o < nops; o++) {
-            if (pos + QSV2_OP_WORDS > nwords) { err = "truncated op record"; return QSV_ERR_BAD_STREAM; }
+            if (pos + opw > nwords) { err = "truncated op record"; return QSV_ERR_BAD_STREAM; }
             const int32_t *rec = seg + pos;
             if (rec[0] != QSV2_OP_MUX2) { err = "unknown opcode " + std::to_string(rec[0]); return QSV_ERR_BAD_STREAM; }
             const int t = rec[1];
@@ -52,9 +67,23 @@ int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPas
                 if ((cm >> b) & 1) op.cmask |= 1ull << phys(b);
             // a control on the target bit can never be set in i0, so M1 is never selected: keep that
             // meaning by recording it (the engine tests i0, which has the target bit clear)
-            for (int e = 0; e < 8; e++) { op.m0[e] = f_of(rec[8 + e]); op.m1[e] = f_of(rec[16 + e]); }
+            if (dtype) {
+                for (int e = 0; e < 8; e++) {
+                    op.d0[e] = d_of(rec + 8 + 2 * e);
+                    op.d1[e] = d_of(rec + 24 + 2 * e);
+                    op.m0[e] = (float)op.d0[e];
+                    op.m1[e] = (float)op.d1[e];
+                }
+            } else {
+                for (int e = 0; e < 8; e++) {
+                    op.m0[e] = f_of(rec[8 + e]);
+                    op.m1[e] = f_of(rec[16 + e]);
+                    op.d0[e] = op.m0[e];
+                    op.d1[e] = op.m1[e];
+                }
+            }
             pp.ops.push_back(op);
-            pos += QSV2_OP_WORDS;
+            pos += opw;
         }
         out.push_back(std::move(pp));
     }
@@ -87,6 +116,13 @@ int layout_for_kw(int kw, int *rb, int *wb) {
     }
 }
 
+int layout_for_kw_c128(int kw, int *rb, int *wb) {
+    if (kw < 10 || kw > 12) return -1;
+    *rb = 4;
+    *wb = kw - 9;
+    return 0;
+}
+
 static uint64_t op_qubits(const PhysOp &op) { return op.cmask | (1ull << op.t); }
 
 static int window_lo(uint64_t qset, int n, int kw) {
@@ -99,20 +135,31 @@ static int window_lo(uint64_t qset, int n, int kw) {
     return best;
 }
 
-static uint8_t classify(const float *m) {
-    auto z = [](float x) { return x == 0.0f; };
+template <class T>
+static uint8_t classify(const T *m) {
+    auto z = [](T x) { return x == (T)0; };
     const bool offz = z(m[2]) && z(m[3]) && z(m[4]) && z(m[5]);
-    if (offz && m[0] == 1.0f && z(m[1]) && m[6] == 1.0f && z(m[7])) return QSV_M_IDENT;
-    if (offz && m[0] == 1.0f && z(m[1])) return QSV_M_DIAG1;
+    if (offz && m[0] == (T)1 && z(m[1]) && m[6] == (T)1 && z(m[7])) return QSV_M_IDENT;
+    if (offz && m[0] == (T)1 && z(m[1])) return QSV_M_DIAG1;
     if (offz) return QSV_M_DIAG;
-    if (z(m[0]) && z(m[1]) && m[2] == 1.0f && z(m[3]) && m[4] == 1.0f && z(m[5]) && z(m[6]) && z(m[7]))
+    if (z(m[0]) && z(m[1]) && m[2] == (T)1 && z(m[3]) && m[4] == (T)1 && z(m[5]) && z(m[6]) && z(m[7]))
         return QSV_M_XSWAP;
     return QSV_M_DENSE;
 }
 
+static void set_mats(QsvOp &o, const PhysOp &p) {
+    std::memcpy(o.m0, p.m0, sizeof(o.m0));
+    std::memcpy(o.m1, p.m1, sizeof(o.m1));
+}
+static void set_mats(QsvOpD &o, const PhysOp &p) {
+    std::memcpy(o.m0, p.d0, sizeof(o.m0));
+    std::memcpy(o.m1, p.d1, sizeof(o.m1));
+}
+
 // Tensor-map staging for windows with short contiguous runs: one dim per chunk (<= 8 bits) of each run of
 // window bits, each spanning the free bits up to the next window bit. Returns the rank, 0 if it does not fit.
-static int tma_dims(const QsvSweep &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart) {
+template <class SW>
+static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart) {
     if (sw.lo >= QSV_TMA_TENSOR_LO) return 0;
     int wb[QSV_KW_MAX], nw = 0;            // window bits ascending
     for (int q = 0; q < sw.lo; q++) wb[nw++] = q;
@@ -134,19 +181,27 @@ static int tma_dims(const QsvSweep &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *
 }
 
 // Ops [b, e) in tile coordinates of a window (tile_of[q] = tile bit of physical qubit q) and their phases.
-// Phases are greedy in op order: tile bits >= 4 that are targets need a register or lane slot.
+// Phases are greedy in op order: tile bits above the fixed lane bits (>= 4 for complex64, whose tile bit 0
+// is the packed half of a float4 and bits 1-3 are lanes; >= 3 for complex128, bits 0-2 lanes) that are
+// targets need a register or lane slot.
+template <class OpT>
 static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n, int kw,
-                       std::vector<QsvOp> &out, std::vector<QsvPhaseX> &phases, std::string &err) {
+                       std::vector<OpT> &out, std::vector<QsvPhaseX> &phases, std::string &err) {
+    constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
+    constexpr int FIXED_LO = C128 ? 0 : 1;       // first tile bit on lane bits 0-2
+    constexpr int FREE_LO = FIXED_LO + 3;        // tile bits from here on need a slot when targeted
     int rb, wb;
-    if (layout_for_kw(kw, &rb, &wb)) { err = "unsupported window size"; return QSV_ERR_UNSUPPORTED; }
-    out.assign(e - b, QsvOp());
+    if (C128 ? layout_for_kw_c128(kw, &rb, &wb) : layout_for_kw(kw, &rb, &wb)) {
+        err = "unsupported window size";
+        return QSV_ERR_UNSUPPORTED;
+    }
+    out.assign(e - b, OpT());
     phases.clear();
     for (size_t i = b; i < e; i++) {
-        QsvOp &o = out[i - b];
+        OpT &o = out[i - b];
         std::memset(&o, 0, sizeof(o));
         const PhysOp &p = ops[i];
-        std::memcpy(o.m0, p.m0, sizeof(o.m0));
-        std::memcpy(o.m1, p.m1, sizeof(o.m1));
+        set_mats(o, p);
         o.tbit = (uint8_t)tile_of[p.t];
         o.cmask = 0;
         for (int q = 0; q < n; q++)
@@ -163,7 +218,7 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
         if (o.cmask == 0) { o.kind = QSV_K_UNI; o.cls = o.cls0; }
         else if (o.cls0 == QSV_M_IDENT) { o.kind = QSV_K_CTRL; o.cls = o.cls1; }
         else { o.kind = QSV_K_MUX; o.cls = QSV_M_DENSE; }
-        o.cm_c = (uint8_t)(o.cmask & 1u);
+        o.cm_c = C128 ? 0 : (uint8_t)(o.cmask & 1u);
         // code path; the dense arithmetic gives the same values on diagonal / permutation matrices
         if (o.kind == QSV_K_UNI) {
             o.variant = o.cls == QSV_M_IDENT ? QSV_V_SKIP
@@ -185,7 +240,7 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
         int used[QSV_KW_MAX], cnt[QSV_KW_MAX], nu = 0;
         while (j < nops) {
             const int tb = out[j].tbit;
-            if (tb >= 4) {
+            if (tb >= FREE_LO) {
                 int f = -1;
                 for (int u = 0; u < nu; u++)
                     if (used[u] == tb) f = u;
@@ -213,7 +268,7 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             else lanes[nl++] = slots[u];
         }
         int rest[QSV_KW_MAX], nrest = 0;
-        for (int t = 4; t < kw; t++)
+        for (int t = FREE_LO; t < kw; t++)
             if (!taken[t]) rest[nrest++] = t;
         int ri = 0;
         while (nr < rb) regs[nr++] = rest[ri++];
@@ -227,10 +282,10 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
         uint32_t regmask = 0;
         for (int r = 0; r < rb; r++) regmask |= 1u << ph.reg_bits[r];
         for (size_t o = i; o < j; o++) {
-            QsvOp &op = out[o];
+            OpT &op = out[o];
             const int tb = op.tbit;
-            if (tb == 0) op.slot = QSV_SLOT_COMP;
-            else if (tb < 4) op.slot = (uint8_t)(QSV_SLOT_LANE0 + tb - 1);
+            if (!C128 && tb == 0) op.slot = QSV_SLOT_COMP;
+            else if (tb < FREE_LO) op.slot = (uint8_t)(QSV_SLOT_LANE0 + tb - FIXED_LO);
             else {
                 op.slot = 0xff;
                 for (int r = 0; r < rb; r++)
@@ -243,10 +298,10 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             op.cm_reg = 0;
             for (int r = 0; r < rb; r++)
                 if ((op.cmask >> ph.reg_bits[r]) & 1) op.cm_reg |= (uint8_t)(1u << r);
-            op.cm_thr = op.cmask & ~regmask & ~1u;
+            op.cm_thr = op.cmask & ~regmask & (C128 ? ~0u : ~1u);
             // controls on lane bits make the selection differ between the lanes of a warp: take the
             // branch-free form of the controlled variants there
-            const uint32_t lanemask = 0xEu | (1u << ph.lane_bits[0]) | (1u << ph.lane_bits[1]);
+            const uint32_t lanemask = (C128 ? 0x7u : 0xEu) | (1u << ph.lane_bits[0]) | (1u << ph.lane_bits[1]);
             if (op.cm_thr & lanemask) {
                 if (op.variant == QSV_V_CTRL_DENSE) op.variant = QSV_V_CTRL_DENSE_SEL;
                 else if (op.variant == QSV_V_CTRL_DIAG1) op.variant = QSV_V_CTRL_DIAG1_SEL;
@@ -259,10 +314,15 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
     return QSV_OK;
 }
 
+template <class OpT>
 static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
-                      QsvSweep &sw, std::string &err) {
+                      QsvSweepT<OpT> &sw, std::string &err) {
+    constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
     int rb, wb;
-    if (layout_for_kw(kw, &rb, &wb)) { err = "unsupported window size"; return QSV_ERR_UNSUPPORTED; }
+    if (C128 ? layout_for_kw_c128(kw, &rb, &wb) : layout_for_kw(kw, &rb, &wb)) {
+        err = "unsupported window size";
+        return QSV_ERR_UNSUPPORTED;
+    }
     std::memset(&sw, 0, sizeof(sw));
     const int lo = window_lo(qset, n, kw);
     if (lo < QSV_LO_MIN) { err = "op qubits do not fit one 13-qubit window"; return QSV_ERR_UNSUPPORTED; }
@@ -277,20 +337,20 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         if ((qset >> q) & 1) { sw.H[nh] = (uint8_t)q; tile_of[q] = lo + nh; nh++; }
     sw.nh = nh;
     sw.ntiles = 1ll << (n - kw);
-    {
+    if (!C128) {       // complex128 tiles are staged with bulk copies only
         uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
         const int r = tma_dims(sw, tfree, tbox, tstart);
         sw.tma_rank = (uint8_t)r;
         for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
     }
-    std::vector<QsvOp> vops;
+    std::vector<OpT> vops;
     std::vector<QsvPhaseX> vph;
-    int rc = plan_window(ops, b, e, tile_of, n, kw, vops, vph, err);
+    int rc = plan_window<OpT>(ops, b, e, tile_of, n, kw, vops, vph, err);
     if (rc) return rc;
     if (vops.size() > QSV_MAX_SWEEP_OPS || vph.size() > QSV_MAX_PHASES) { err = "sweep too large"; return QSV_ERR_UNSUPPORTED; }
     sw.nops = (int)vops.size();
     sw.nphases = (int)vph.size();
-    std::memcpy(sw.ops, vops.data(), vops.size() * sizeof(QsvOp));
+    std::memcpy(sw.ops, vops.data(), vops.size() * sizeof(OpT));
     for (size_t p = 0; p < vph.size(); p++) {
         QsvPhase &d = sw.phases[p];
         const QsvPhaseX &x = vph[p];
@@ -309,11 +369,12 @@ int plan_whole_state(const std::vector<PhysPass> &passes, int n, std::vector<Qsv
     for (const PhysPass &p : passes) ops.insert(ops.end(), p.ops.begin(), p.ops.end());
     int tile_of[64];
     for (int q = 0; q < 64; q++) tile_of[q] = q < n ? q : -1;
-    return plan_window(ops, 0, ops.size(), tile_of, n, n, ops_out, phases_out, err);
+    return plan_window<QsvOp>(ops, 0, ops.size(), tile_of, n, n, ops_out, phases_out, err);
 }
 
-int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge, std::vector<QsvSweep> &out,
-                 std::string &err) {
+template <class OpT>
+int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merge,
+                 std::vector<QsvSweepT<OpT>> &out, std::string &err) {
     out.clear();
     std::vector<PhysOp> ops;
     uint64_t cur = 0;
@@ -321,7 +382,7 @@ int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merg
     auto flush = [&]() -> int {
         if (ops.size() > begin) {
             out.emplace_back();
-            int rc = fill_sweep(ops, begin, ops.size(), cur, n, kw, out.back(), err);
+            int rc = fill_sweep<OpT>(ops, begin, ops.size(), cur, n, kw, out.back(), err);
             if (rc) return rc;
         }
         begin = ops.size();
@@ -344,6 +405,10 @@ int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merg
     }
     return flush();
 }
+template int build_sweeps<QsvOp>(const std::vector<PhysPass> &, int, int, int, std::vector<QsvSweep> &,
+                                 std::string &);
+template int build_sweeps<QsvOpD>(const std::vector<PhysPass> &, int, int, int, std::vector<QsvSweepD> &,
+                                  std::string &);
 
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
     std::vector<int32_t> w;

@@ -29,6 +29,8 @@ __device__ int g_status = 0;
 // The interpreter: the sweep's phases and ops are read at run time (op table in shared memory), one code
 // path per op variant selected by a switch.
 struct InterpBody {
+    using Amp = float2;
+    static constexpr int kHalfBits = 1;
     static constexpr bool kSmemOps = true;
     template <int NV, int RB, int WB>
     static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane, int warp,
@@ -87,7 +89,7 @@ cudaError_t make_tmap(CUtensorMap *map, float2 *state, const QsvSweep &sw) {
 template <int KW, int RB, int WB, int S>
 static cudaError_t launch_sweep_t(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream) {
     constexpr int NT = (1 << (5 + WB)) + 32;
-    const size_t smem = sweep_smem_bytes<KW, S>(InterpBody::kSmemOps);
+    const size_t smem = sweep_smem_bytes<KW, S, InterpBody>();
     static int configured_dev = -1;     // attribute set once per device (under the engine's launch lock)
     static int per_sm = 1;
     int dev = 0;

@@ -65,26 +65,32 @@ __device__ __forceinline__ void tma_store(const CUtensorMap *map, const int32_t 
 }
 
 // Dynamic shared memory a sweep kernel needs: S tile buffers, plus the op table when Body reads it there.
-template <int KW, int S>
-__host__ __device__ constexpr size_t sweep_smem_bytes(bool smem_ops) {
-    return ((size_t)S << KW) * 8 + (smem_ops ? sizeof(QsvOp) * QSV_MAX_SWEEP_OPS : 0);
+template <int KW, int S, class Body, class SW = QsvSweep>
+__host__ __device__ constexpr size_t sweep_smem_bytes() {
+    return ((size_t)S << KW) * sizeof(typename Body::Amp) +
+           (Body::kSmemOps ? sizeof(typename SW::op_type) * QSV_MAX_SWEEP_OPS : 0);
 }
 
-// The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S>(Body::kSmemOps)
-// bytes of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
-template <int KW, int RB, int WB, int S, int G, class Body>
-__device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const QsvSweep &P, const CUtensorMap *tmap,
-                                               int *status) {
+// The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S, Body, SW>() bytes
+// of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
+// Body::Amp is the amplitude type (float2: complex64, double2: complex128); Body::kHalfBits is 1 when a
+// thread's 16-byte slot packs two amplitudes (tile bit 0), 0 when it holds one.
+template <int KW, int RB, int WB, int S, int G, class Body, class SW = QsvSweep>
+__device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ state, const SW &P,
+                                               const CUtensorMap *tmap, int *status) {
+    using Amp = typename Body::Amp;
+    using Op = typename SW::op_type;
     constexpr int NCG = 1 << (5 + WB);       // consumer threads of one group
     constexpr int NC = G * NCG;              // consumer threads
-    constexpr int NV = 1 << RB;              // float4 per consumer thread
+    constexpr int NV = 1 << RB;              // 16-byte slots per consumer thread
     constexpr int TILE = 1 << KW;            // amplitudes per tile
-    static_assert(1 + 3 + 2 + RB + WB == KW, "layout must cover the window");
+    constexpr uint32_t TILE_BYTES = (uint32_t)TILE * (uint32_t)sizeof(Amp);
+    static_assert(Body::kHalfBits + 3 + 2 + RB + WB == KW, "layout must cover the window");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    float2 *bufs = reinterpret_cast<float2 *>(smem_raw);
+    Amp *bufs = reinterpret_cast<Amp *>(smem_raw);
     // the interpreter's op table, copied once from the parameter block: shared-memory reads of an op's
     // fields are independent short-latency loads (the constant-bank path serialises run-time indices)
-    QsvOp *sops = reinterpret_cast<QsvOp *>(smem_raw + ((size_t)S << KW) * sizeof(float2));
+    Op *sops = reinterpret_cast<Op *>(smem_raw + ((size_t)S << KW) * sizeof(Amp));
     // full barrier of tile j: full[j % (S * G)]. Tiles sharing a full barrier share a buffer (j % S) and a
     // consumer group (j % G), so each full barrier is waited on by one group, phase after phase (a parity
     // wait never meets a phase two steps old). done[b] is waited on by the producer alone, tile by tile.
@@ -97,7 +103,7 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
     if (Body::kSmemOps) {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(P.ops);
         uint32_t *dst = reinterpret_cast<uint32_t *>(sops);
-        const int words = P.nops * (int)(sizeof(QsvOp) / 4);
+        const int words = P.nops * (int)(sizeof(Op) / 4);
         for (int i = tid; i < words; i += blockDim.x) dst[i] = src[i];
     }
     if (tid == 0) {
@@ -126,7 +132,7 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
             }
         };
         const int nsub = 1 << (KW - lo);
-        const uint32_t subbytes = 8u << lo;
+        const uint32_t subbytes = (uint32_t)sizeof(Amp) << lo;
         const int nh = P.nh;
         auto tile_base = [&](int64_t T) -> int64_t {
             int64_t x = T << lo;                      // free bits are the bits outside [0, lo) U H
@@ -144,25 +150,25 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
         };
         auto issue_load = [&](int64_t j, int b) {
             const int64_t T = first + j * stride;
-            float2 *dst = bufs + (size_t)b * TILE;
+            Amp *dst = bufs + (size_t)b * TILE;
             uint64_t *fb = &full[j % NF];
             if (rank) {
                 if (lane == 0) {
                     int32_t c[QSV_TMA_MAX_RANK];
                     coords(T, c);
-                    mbar_arrive_expect_tx(fb, (uint32_t)TILE * 8u);
+                    mbar_arrive_expect_tx(fb, TILE_BYTES);
                     tma_load(dst, tmap, c, rank, fb);
                 }
                 return;
             }
             const int64_t base = tile_base(T);
-            if (lane == 0) mbar_arrive_expect_tx(fb, (uint32_t)TILE * 8u);
+            if (lane == 0) mbar_arrive_expect_tx(fb, TILE_BYTES);
             __syncwarp();
             for (int s = lane; s < nsub; s += 32) bulk_g2s(dst + (s << lo), state + (base | sub_off(s)), subbytes, fb);
         };
         auto issue_store = [&](int64_t j, int b) {
             const int64_t T = first + j * stride;
-            const float2 *src = bufs + (size_t)b * TILE;
+            const Amp *src = bufs + (size_t)b * TILE;
             if (rank) {
                 if (lane == 0) {
                     int32_t c[QSV_TMA_MAX_RANK];
@@ -199,7 +205,7 @@ __device__ __forceinline__ void sweep_pipeline(float2 *__restrict__ state, const
         const int b = (int)(j % S);
         const uint32_t par = (uint32_t)((j / NF) & 1);
         if (!mbar_wait(&full[j % NF], par, &abort_flag, status)) break;
-        float2 *tile = bufs + (size_t)b * TILE;
+        Amp *tile = bufs + (size_t)b * TILE;
         Body::template tile<NV, RB, WB>(tile, P, sops, lane, warp, 1 + grp);
         fence_proxy_async_smem();
         mbar_arrive(&done[b]);

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libqsv_b200.so")
 
 QSV_OK = 0
 QSV_C64 = 0
+QSV_C128 = 1            # complex128 states with FP64-matrix segments (header word 4 = 1)
 CHUNK_BITS = 12
 N_MIN, N_MAX = 10, 34
 
@@ -122,25 +123,41 @@ def _qubits(state):
     return n
 
 
-def new_state(n, device=None, zero=True, stream=None):
-    """Allocate a complex64 device state of 2^n amplitudes (|0...0> unless zero=False)."""
+def _dt(state):
+    """Element-type code of a state tensor: QSV_C64 (complex64) or QSV_C128 (complex128)."""
     torch = _torch()
-    t = torch.empty(1 << n, dtype=torch.complex64, device=device or "cuda")
+    if state.dtype == torch.complex64:
+        return QSV_C64
+    if state.dtype == torch.complex128:
+        return QSV_C128
+    raise TypeError(f"states are complex64 or complex128 tensors, not {state.dtype}")
+
+
+def new_state(n, device=None, zero=True, stream=None, dtype=None):
+    """Allocate a device state of 2^n amplitudes (complex64 unless dtype=torch.complex128 or "c128";
+    |0...0> unless zero=False)."""
+    torch = _torch()
+    if dtype in (None, "c64"):
+        dtype = torch.complex64
+    elif dtype == "c128":
+        dtype = torch.complex128
+    t = torch.empty(1 << n, dtype=dtype, device=device or "cuda")
     if zero:
         zero_state(t, stream)
     return t
 
 
 def zero_state(state, stream=None):
-    _check(load().qsv_zero_state(_ptr(state), _qubits(state), QSV_C64, _stream(stream)))
+    _check(load().qsv_zero_state(_ptr(state), _qubits(state), _dt(state), _stream(stream)))
 
 
 def run_segment(state, seg, stream=None):
-    """Execute one QSV2 segment (np.int32 words) in place on a complex64 CUDA tensor."""
-    assert state.is_cuda and state.dtype.is_complex and state.element_size() == 8 and state.is_contiguous()
+    """Execute one QSV2 segment (np.int32 words) in place on a CUDA state: complex64 with a reference
+    format segment, complex128 with an FP64-matrix segment (compile_circuit(..., dtype="c128"))."""
+    assert state.is_cuda and state.is_contiguous()
     w = np.ascontiguousarray(seg, dtype=np.int32)
     _check(load().qsv_run_segment(_ptr(state), _qubits(state), w.ctypes.data_as(ctypes.c_void_p), w.size,
-                                  QSV_C64, _stream(stream)))
+                                  _dt(state), _stream(stream)))
 
 
 def remap(src, dst, perm, stream=None):
@@ -149,7 +166,9 @@ def remap(src, dst, perm, stream=None):
     n = _qubits(src)
     if len(p) != n or dst.numel() != src.numel():
         raise ValueError("permutation length / state size mismatch")
-    _check(load().qsv_remap(_ptr(src), _ptr(dst), n, p.ctypes.data_as(ctypes.c_void_p), QSV_C64, _stream(stream)))
+    if dst.dtype != src.dtype:
+        raise ValueError("remap source and destination differ in element type")
+    _check(load().qsv_remap(_ptr(src), _ptr(dst), n, p.ctypes.data_as(ctypes.c_void_p), _dt(src), _stream(stream)))
 
 
 def scratch_bytes(n):
@@ -167,7 +186,8 @@ def reduce_f64(state, out=None, scratch=None, stream=None):
     n = _qubits(state)
     out = torch.empty(n + 1, dtype=torch.float64, device=state.device) if out is None else out
     scratch = new_scratch(n, state.device) if scratch is None else scratch
-    _check(load().qsv_reduce_f64(_ptr(state), n, QSV_C64, _ptr(out), _ptr(scratch), scratch.numel(), _stream(stream)))
+    _check(load().qsv_reduce_f64(_ptr(state), n, _dt(state), _ptr(out), _ptr(scratch), scratch.numel(),
+                                 _stream(stream)))
     return out
 
 
@@ -175,7 +195,7 @@ def chunk_probs_f64(state, chunk_bits=CHUNK_BITS, stream=None):
     torch = _torch()
     n = _qubits(state)
     out = torch.empty(1 << (n - chunk_bits), dtype=torch.float64, device=state.device)
-    _check(load().qsv_chunk_probs_f64(_ptr(state), n, QSV_C64, chunk_bits, _ptr(out), _stream(stream)))
+    _check(load().qsv_chunk_probs_f64(_ptr(state), n, _dt(state), chunk_bits, _ptr(out), _stream(stream)))
     return out
 
 
@@ -187,7 +207,7 @@ def sample_f64(state, uniforms, scratch=None, stream=None):
     u = u.to(device=state.device, dtype=torch.float64).contiguous()
     out = torch.empty(u.numel(), dtype=torch.int64, device=state.device)
     scratch = new_scratch(n, state.device) if scratch is None else scratch
-    _check(load().qsv_sample_f64(_ptr(state), n, QSV_C64, _ptr(u), u.numel(), _ptr(out), _ptr(scratch),
+    _check(load().qsv_sample_f64(_ptr(state), n, _dt(state), _ptr(u), u.numel(), _ptr(out), _ptr(scratch),
                                  scratch.numel(), _stream(stream)))
     return out
 

@@ -48,10 +48,11 @@ def logical_counts(phys, fmap, n):
 
 class SVRuntime:
     """One GPU. The FPGA-specific constructor arguments of the reference (bdf, xclbin, n_engines, n_swap,
-    use_device_swap) are accepted and ignored so call sites keep working."""
+    use_device_swap) are accepted and ignored so call sites keep working. dtype="c128" (no reference
+    counterpart) runs complex128 states with FP64 matrices, the on-GPU FP64 path."""
 
     def __init__(self, bdf=None, xclbin=None, n_engines=None, n_swap=0, use_device_swap=True, max_high=None,
-                 device=None):
+                 device=None, dtype="c64"):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("SVRuntime needs a CUDA device (B200); none is available")
@@ -61,6 +62,9 @@ class SVRuntime:
         if max_high is not None and max_high > MAX_HIGH:
             raise ValueError(f"max_high={max_high} exceeds the QSV2 pass header's {MAX_HIGH} slots")
         self.max_high = MAX_HIGH if max_high is None else max_high
+        if dtype not in ("c64", "c128"):
+            raise ValueError(f"dtype must be 'c64' or 'c128', not {dtype!r}")
+        self.dtype = dtype
         self.stream = torch.cuda.current_stream(self.device)
         self.L = None
         self.P = 1
@@ -84,7 +88,8 @@ class SVRuntime:
             return
         self.st = self.alt = self.scratch = None
         torch.cuda.empty_cache()
-        self.st = torch.empty(1 << L, dtype=torch.complex64, device=self.device)
+        self.st = torch.empty(1 << L, dtype=torch.complex128 if self.dtype == "c128" else torch.complex64,
+                              device=self.device)
         self.scratch = engine.new_scratch(L, self.device)
         self.L = L
 
@@ -115,7 +120,7 @@ class SVRuntime:
         else:
             qrun = qc.remove_final_measurements(inplace=False)
         prog, fmap, stats = compile_circuit(qrun, L, k, fuse_1q=fuse, tiling=tiling, initial_map=initial_map,
-                                            max_high=self.max_high)
+                                            max_high=self.max_high, dtype=self.dtype)
         t1 = time.perf_counter()
         self._alloc(L)
         t1b = time.perf_counter()
