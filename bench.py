@@ -161,6 +161,31 @@ def cpu_sample(seg, n, n_tiles_total, seconds=12.0, workers=None):
     return moved / busy / 1e9, workers, desc, wall
 
 
+# ------------------------------------------------------------------ precision study
+def precision_main(a):
+    """One JSON line: Run A (33 qubits, complex64) and Run B (32 qubits, complex128 against complex64)
+    of the random-layer circuit with CZ brickwork and Toffolis, depth 16, seed 2."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    pkg = _package()
+    import torch
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    precision = import_module("qsv_b200.precision")
+    engine.load()
+    torch.cuda.set_device(0)
+    n_a = a.n if a.n != 30 else 33
+    res = precision.study(n_a=n_a, n_b=n_a - 1, depth=16, seed=2)
+    rb = res["run_b"]
+    sweeps_bytes = 32 << rb["n"]
+    print(json.dumps({"metric": "precision study: 1-F of complex64 vs complex128 (on-GPU FP64)",
+                      "value": rb["c64_vs_c128"]["one_minus_f"], "unit": "1-F", "higher_is_better": False,
+                      "n_gpus": 1, "dtype": "c64 and c128", "data": "synthetic (seeded circuit)",
+                      "config": {"workload": f"random_layer_ccx depth 16 seed 2: run A {n_a}q complex64, "
+                                             f"run B {n_a - 1}q complex128 vs complex64"},
+                      "runs": res}))
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -175,7 +200,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
                     help="specialised sweep kernels (compiled before the warm-up unless off)")
+    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision"],
+                    help="rl30: the headline sweep benchmark; precision: the complex64 / complex128 study "
+                         "(33 qubits complex64, 32 qubits complex128 vs complex64)")
     a = ap.parse_args()
+    if a.workload == "precision":
+        return precision_main(a)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -68,3 +68,27 @@ def test_jit_mode_switch(lib):
             engine.set_jit(7)
     finally:
         engine.set_jit(old)
+
+
+def test_exit_with_compilations_in_flight():
+    """A process that exits while specialised kernels are compiling in the background exits cleanly."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, threading, time\n"
+        f"sys.path.insert(0, {os.path.join(root, 'tests')!r}); sys.path.insert(0, {root!r})\n"
+        "import conftest\n"
+        "import qsv_b200 as q\n"
+        "from qsv_b200 import engine, generators as gen\n"
+        "prog, _, _ = q.compile_circuit(gen.qft(20), 20, 12)\n"
+        "segs = [s for k, s in prog if k == 'segment']\n"
+        "def bg():\n"
+        "    for s in segs: engine.jit_prepare(s, 20)\n"
+        "threading.Thread(target=bg, daemon=True).start()\n"
+        "time.sleep(0.5)\n"
+        "assert engine.jit_info()['pending'] > 0\n"
+    )
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]

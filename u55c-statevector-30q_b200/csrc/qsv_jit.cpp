@@ -104,6 +104,7 @@ struct Jit {
     std::unordered_map<std::string, std::shared_ptr<Entry>> map;
     std::deque<std::shared_ptr<Entry>> queue;
     int threads = 0, busy = 0;
+    bool stopping = false;      // set at process exit: workers take no new work
     int mode = 2;
     long long jit_launches = 0, interp_launches = 0, compiled = 0, failed = 0;
     double compile_ms = 0.0;
@@ -227,7 +228,12 @@ void worker() {
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
     for (;;) {
-        j.work.wait(lk, [&] { return !j.queue.empty(); });
+        j.work.wait(lk, [&] { return j.stopping || !j.queue.empty(); });
+        if (j.stopping) {
+            // park for good: a thread that exits during process teardown runs its thread-local destructors
+            // after the libraries it used may be gone
+            j.work.wait(lk, [] { return false; });
+        }
         std::shared_ptr<Entry> e = j.queue.front();
         j.queue.pop_front();
         j.busy++;
@@ -251,13 +257,50 @@ void worker() {
     }
 }
 
+// Drop queued compilations and wait (up to 60 s) for running ones; with j.mu held by lk.
+void drain(Jit &j, std::unique_lock<std::mutex> &lk) {
+    for (auto &e : j.queue) e->state = kNew;
+    j.queue.clear();
+    j.done.notify_all();
+    j.done.wait_for(lk, std::chrono::seconds(60), [&] { return j.busy == 0; });
+}
+
+// Process exit with a compilation in flight would tear NVRTC down under a running compile. This handler
+// drops the queue and waits for running compilations to finish. It is registered after a first (tiny)
+// compilation has loaded NVRTC's run-time parts, so that it runs before their teardown (exit handlers
+// run in reverse order of registration).
+void stop_workers_at_exit() {
+    Jit &j = J();
+    std::unique_lock<std::mutex> lk(j.mu);
+    j.stopping = true;
+    j.work.notify_all();
+    drain(j, lk);
+}
+
+void warm_up_nvrtc() {
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, "extern \"C\" __global__ void qsv_warm_up() {}\n", "warm_up.cu", 0, nullptr,
+                           nullptr) != NVRTC_SUCCESS)
+        return;
+    const char *opts[] = {"--gpu-architecture=sm_100a", "-std=c++17"};
+    nvrtcCompileProgram(prog, 2, opts);
+    nvrtcDestroyProgram(&prog);
+}
+
 // with j.mu held: queue e for compilation (starts the compile threads on first use)
 void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
     if (e->state != kNew) return;
     e->src = gen_source(sw, e->rb, e->wb);
     e->state = kQueued;
     j.queue.push_back(e);
+    if (j.stopping) {
+        e->state = kNew;
+        j.queue.pop_back();
+        return;
+    }
     if (j.threads == 0) {
+        warm_up_nvrtc();
+        std::atexit(stop_workers_at_exit);
         const unsigned hw = std::thread::hardware_concurrency();
         const int n = std::max(1, std::min(8, (int)(hw ? hw / 2 : 2)));
         for (int i = 0; i < n; i++) std::thread(worker).detach();
@@ -283,9 +326,10 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
 int jit_set_mode(int mode) {
     if (mode < 0 || mode > 2) return -1;
     Jit &j = J();
-    std::lock_guard<std::mutex> lk(j.mu);
+    std::unique_lock<std::mutex> lk(j.mu);
     const int old = j.mode;
     j.mode = mode;
+    if (mode == 0) drain(j, lk);       // interpreter only: queued compilations are dropped
     return old;
 }
 
@@ -315,7 +359,7 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
 void jit_wait() {
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
-    j.done.wait(lk, [&] { return j.queue.empty() && j.busy == 0; });
+    j.done.wait(lk, [&] { return (j.queue.empty() && j.busy == 0) || j.stopping; });
 }
 
 // stats: mode, structures, ready, failed, launches specialised, launches interpreted, compile ms, queued

@@ -77,6 +77,10 @@ def load(path=LIB_PATH):
         f.argtypes = args
         f.restype = res
     _lib = L
+    # before the interpreter shuts down: drop queued specialised-kernel compilations and let running ones
+    # finish (the library also does this from its own exit handler)
+    import atexit
+    atexit.register(L.qsv_set_jit, 0)
     return L
 
 
