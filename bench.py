@@ -35,8 +35,9 @@ PKG_DIR = os.path.join(ROOT, "u55c-statevector-30q_b200")
 METRIC = "30q pass sweep GB/s (random-layer d24)"
 HBM_FALLBACK_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum per sweep launch over the algorithmic 16 B x 2^n, measured
-# with ncu on the 26-qubit version of this workload (72 launches, median); traffic grows as 2^n
-TRAFFIC_PER_ALGORITHMIC = 0.943
+# with ncu on the 26-qubit version of this workload (specialised kernels, three launches: 1013-1015 MB of
+# 1074 MB); traffic grows as 2^n
+TRAFFIC_PER_ALGORITHMIC = 0.944
 
 
 def _package():
@@ -186,6 +187,100 @@ def precision_main(a):
                       "runs": res}))
 
 
+# ------------------------------------------------------------------ batched and served workloads
+def batched_main(a):
+    """Batched: `count` circuits (qubits uniform in [10, 24], depths in [5, 40], U3 / CZ / Toffoli layers,
+    circuit i seeded 3 + i) per replay of one captured CUDA graph, against the plain one-circuit-at-a-time
+    path on the same compiled programs; results must be identical. Device work only (programs compiled
+    before timing, in spawned workers); host compile time reported beside."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    pkg = _package()
+    import torch
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    batch = import_module("qsv_b200.batch")
+    engine.load()
+    torch.cuda.set_device(0)
+    engine.set_jit(a.jit)
+    count = a.count or 512
+    circs = batch.config4_circuits(count=count)
+    t0 = time.perf_counter()
+    progs = batch.compile_many(circs, workers=min(16, os.cpu_count() or 1))
+    t_compile = time.perf_counter() - t0
+    br = batch.BatchRunner(streams=8, autotune=True)
+    plan = br.prepare(circs, programs=progs)
+    br.capture(plan)
+    for _ in range(max(1, a.warmup)):
+        br.run(plan)
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(a.steps):
+            t = time.perf_counter()
+            z, states = br.run(plan)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t)
+    t_plain = time.perf_counter()
+    zp = batch.plain_run(circs, progs)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t_plain
+    equal = all(x[0] == y[0] and np.array_equal(x[1], y[1]) for x, y in zip(z, zp))
+    t_b = statistics.median(times)
+    print(json.dumps({"metric": "batched circuits/s (CUDA-graph replay) vs plain one-at-a-time",
+                      "value": count / t_b, "unit": "circuits/s", "higher_is_better": True, "n_gpus": 1,
+                      "steps": a.steps, "warmup": a.warmup, "dtype": "c64 (fp32 arithmetic)",
+                      "data": "synthetic (seeded circuits)",
+                      "config": {"workload": f"{count} circuits, n uniform in [10, 24], depth uniform in [5, 40], "
+                                             "U3 / CZ brickwork / Toffoli layers, seeds 3 + i"},
+                      "plain_circuits_per_s": count / t_plain, "speedup_vs_plain": t_plain / t_b,
+                      "batched_s": t_b, "plain_s": t_plain, "results_identical": equal,
+                      "graph_launches": plan.launches, "host_compile_s": t_compile,
+                      "specialised_kernels": engine.jit_info(), "clocks": clk.summary()}))
+
+
+def served_main(a):
+    """Served: Poisson arrivals (rate per second) of circuits with qubit counts log-uniform in [12, qmax]
+    and depths uniform in [10, 100] (U3 / CZ / Toffoli layers, request i seeded 4 + i), admitted under a
+    160 GB HBM budget with continuous batching, against the plain sequential path on the same requests.
+    Programs are compiled before the run (spawned workers), so both sides time device work and queueing."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    pkg = _package()
+    import torch
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    serve = import_module("qsv_b200.serve")
+    engine.load()
+    torch.cuda.set_device(0)
+    engine.set_jit(a.jit)
+    count = a.count or 400
+    workers = min(16, os.cpu_count() or 1)
+    reqs = serve.precompile(serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax), workers=workers)
+    srv = serve.Server(budget_bytes=160e9, max_inflight=16)
+    with ClockSampler(0) as clk:
+        t = time.perf_counter()
+        done = srv.run(reqs)
+        t_served = time.perf_counter() - t
+    srv.close()
+    st = serve.latency_stats(done)
+    reqs2 = serve.precompile(serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax), workers=workers)
+    t = time.perf_counter()
+    plain = serve.plain_serve(reqs2)
+    t_plain = time.perf_counter() - t
+    sp = serve.latency_stats(plain)
+    res = {r.rid: r.result for r in done}
+    equal = all(res[r.rid][0] == r.result[0] and np.array_equal(res[r.rid][1], r.result[1]) for r in plain)
+    print(json.dumps({"metric": "served circuits/s and p50/p99 latency vs plain sequential",
+                      "value": st["circuits_per_s"], "unit": "circuits/s", "higher_is_better": True,
+                      "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)", "data": "synthetic (seeded requests)",
+                      "config": {"workload": f"{count} Poisson arrivals at {a.rate}/s, n log-uniform in "
+                                             f"[12, {a.qmax}], depth uniform in [10, 100], 160 GB HBM budget"},
+                      "served": dict(st, wall_s=t_served, **srv.stats), "plain": dict(sp, wall_s=t_plain),
+                      "speedup_vs_plain": st["circuits_per_s"] / sp["circuits_per_s"],
+                      "results_identical_alone_and_in_mix": equal, "clocks": clk.summary()}))
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -200,12 +295,21 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
                     help="specialised sweep kernels (compiled before the warm-up unless off)")
-    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision"],
+    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served"],
                     help="rl30: the headline sweep benchmark; precision: the complex64 / complex128 study "
-                         "(33 qubits complex64, 32 qubits complex128 vs complex64)")
+                         "(33 qubits complex64, 32 qubits complex128 vs complex64); batched: 512 circuits of "
+                         "10..24 qubits per CUDA-graph replay vs one at a time; served: Poisson arrivals of "
+                         "12..30-qubit circuits, continuous batching vs the plain sequential path")
+    ap.add_argument("--count", type=int, default=0, help="circuits (batched: 512; served: 400)")
+    ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
+    ap.add_argument("--qmax", type=int, default=24, help="served: largest qubit count")
     a = ap.parse_args()
     if a.workload == "precision":
         return precision_main(a)
+    if a.workload == "batched":
+        return batched_main(a)
+    if a.workload == "served":
+        return served_main(a)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -333,7 +437,10 @@ def main():
                                        else "qsv::dev::sweep_kernel<13,4,3,3>" if jit_launches == 0
                                        else f"qsv_sweep_jit x{jit_launches} + sweep_kernel x{launches - jit_launches}"),
                             "algorithmic_bytes_per_launch": bytes_per_sweep},
-               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+               # the reference's own formula (analysis/make_tables.py:321): QSV2 passes x 16 B x 2^n over
+               # the kernel time; above the HBM roofline because consecutive passes share one sweep here
+               "reference_formula_gbs": stats.n_passes * bytes_per_sweep * a.steps * world / sec / 1e9}
         print(json.dumps(out))
     if dist:
         dist.barrier()

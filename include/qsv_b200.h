@@ -146,7 +146,7 @@ QSV_API int qsv_set_lo_merge(int lo);
 QSV_API int qsv_set_layout13(int rb);
 
 /* Tuning knob (no reference counterpart): how many op targets a phase may place on lane bits (warp
- * shuffles) instead of starting a new phase, 0..2 (default 2). Values are identical either way. */
+ * shuffles) instead of starting a new phase, 0..2 (default 1). Values are identical either way. */
 QSV_API int qsv_set_phase_lanes(int k);
 
 /* Specialised sweep kernels (no reference counterpart; the reference's engine is one fixed HLS kernel).
@@ -154,8 +154,10 @@ QSV_API int qsv_set_phase_lanes(int k);
  * sm_100a) for the sweep's structure: its phase layouts and, per op, target slot, code variant and control
  * masks (everything but the matrices and the window). Values are identical either way.
  * mode 0 = interpreter only; 1 = eager: a new structure is compiled (blocking) before its first launch;
- * 2 = automatic (default): a structure is compiled in background threads once it has been launched twice,
- * and used from the first launch after its kernel is ready. Returns the previous mode. Process-wide. */
+ * 2 = automatic (default): a structure is compiled in background threads once its launches have swept
+ * 2^31 amplitudes in total (two sweeps of a 30-qubit state, 512 of a 22-qubit one; at most 64 compilations
+ * wait at a time), and used from the first launch after its kernel is ready. Switching to mode 0 drops
+ * waiting compilations and waits for running ones. Returns the previous mode. Process-wide. */
 QSV_API int qsv_set_jit(int mode);
 
 /* Compile, in parallel and blocking, the specialised kernels of every sweep of a segment for an n-qubit

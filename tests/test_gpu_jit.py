@@ -124,20 +124,25 @@ def test_specialised_equals_interpreter_large(torch, jit_mode):
 
 @pytest.mark.timeout(900)
 def test_auto_mode_switches_without_changing_values(torch, jit_mode):
-    n = 20
-    jit_mode("auto")
+    """Automatic mode compiles a structure once its launches have swept 2^31 amplitudes (here: 32 sweeps
+    of a 26-qubit state) and switches to it between runs; every run equals the interpreter's."""
+    n = 26
     prog, _, _ = q.compile_circuit(gen.random_layer(n, 12, 77), n, 12)
     segs = [s for kind, s in prog if kind == "segment"]
-    x = _rand_state(n, 5)
-    ref = x.copy()
+    x = torch.from_numpy(_rand_state(n, 5)).cuda()
+    jit_mode("off")
+    ref = x.clone()
     for s in segs:
-        orc.run_segment(ref, s)
-    for it in range(4):
-        t = torch.from_numpy(x.copy()).cuda()
+        engine.run_segment(ref, s)
+    jit_mode("auto")
+    before = engine.jit_info()["jit_launches"]
+    for it in range(6):
+        t = x.clone()
         for s in segs:
             engine.run_segment(t, s)
         torch.cuda.synchronize()
-        assert np.array_equal(t.cpu().numpy(), ref), it
+        assert torch.equal(t, ref), it
         engine.jit_wait()
     info = engine.jit_info()
-    assert info["failed"] == 0 and info["jit_launches"] > 0
+    assert engine.device_status() == 0
+    assert info["failed"] == 0 and info["jit_launches"] > before

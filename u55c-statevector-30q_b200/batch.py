@@ -62,7 +62,7 @@ class Autotuner:
     """Per qubit count, the (lo_merge, layout13, phase_lanes) knobs with the lowest measured device time
     on a representative program. Values never depend on the knobs (tested); only speed does."""
 
-    CANDIDATES = [(4, 4, 2), (4, 3, 2), (4, 4, 1), (6, 4, 2), (9, 4, 2)]
+    CANDIDATES = [(4, 4, 1), (4, 3, 1), (4, 4, 2), (4, 4, 0), (6, 4, 1), (9, 4, 1)]   # first = the defaults
 
     def __init__(self, reps=2):
         self.reps = reps
@@ -81,7 +81,7 @@ class Autotuner:
         if n in self.best:
             return self.best[n]
         if n <= SMALL_MAX:
-            self.best[n] = (4, 4, 2)
+            self.best[n] = self.CANDIDATES[0]
             return self.best[n]
         state = engine.new_state(n)
         res = {}

@@ -11,8 +11,10 @@
 // addressing stay kernel parameters. Specialised and interpreted sweeps compute the same values.
 //
 // Modes: 0 = interpreter only; 1 = eager (a new structure is compiled before its first launch);
-// 2 = automatic (default): a structure is compiled in the background once it has been launched
-// kThreshold times, and launches use the interpreter until its kernel is ready.
+// 2 = automatic (default): a structure is compiled in the background once the amplitudes its launches
+// have swept add up to kWorkThreshold (a compilation costs about a second of one host core, worth it
+// for sweeps that run often or over large states), with at most kMaxQueued compilations waiting;
+// launches use the interpreter until the kernel is ready.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -43,7 +45,8 @@ cudaError_t status_word_ptr(int **out);
 
 namespace {
 
-constexpr int kThreshold = 2;      // launches of a structure before automatic mode compiles it
+constexpr double kWorkThreshold = 2147483648.0;   // 2^31 amplitudes: 2 sweeps at 30 qubits, 512 at 22
+constexpr size_t kMaxQueued = 64;
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
 
@@ -94,6 +97,7 @@ struct Entry {
     std::vector<char> cubin;
     std::string log;
     long long uses = 0;
+    double work = 0.0;          // amplitudes swept by this structure's launches
     CUfunction fn[kMaxDevices] = {nullptr};
     int per_sm[kMaxDevices] = {0};
 };
@@ -394,7 +398,10 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
         if (j.mode == 0 || !d.ok) { j.interp_launches++; return 0; }
         e = find_or_add(j, sw, rb, wb);
         e->uses++;
-        if (e->state == kNew && (j.mode == 1 || e->uses >= kThreshold)) enqueue(j, e, sw);
+        e->work += (double)sw.ntiles * (double)(1 << sw.kw);
+        if (e->state == kNew &&
+            (j.mode == 1 || (e->work >= kWorkThreshold && j.queue.size() < kMaxQueued)))
+            enqueue(j, e, sw);
         if (j.mode == 1) j.done.wait(lk, [&] { return e->state != kQueued; });
         if (e->state != kReady) { j.interp_launches++; return 0; }
     }

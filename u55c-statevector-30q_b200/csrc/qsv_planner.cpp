@@ -92,7 +92,9 @@ int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPas
 }
 
 static int g_rb13 = 4;      // register bits of the 13-qubit layout: 4 (256 consumer threads) or 3 (512)
-static int g_phase_lanes = 2;   // targets (tile bits >= 4) a phase may place on lane bits 3, 4 (0..2)
+// targets (tile bits >= 4) a phase may place on lane bits 3, 4 (0..2). 1 measured fastest on the 30-qubit
+// random-layer program (interpreter and specialised kernels); 0 on the 30-qubit QFT
+static int g_phase_lanes = 1;
 
 int set_phase_lanes(int k) {
     if (k < 0 || k > 2) return -1;

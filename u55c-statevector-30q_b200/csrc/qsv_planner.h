@@ -37,7 +37,7 @@ int decode_segment(const int32_t *seg, size_t nwords, int n, std::vector<PhysPas
 int layout_for_kw(int kw, int *rb, int *wb);
 // Choose the 13-qubit layout: 4 register bits x 8 consumer warps, or 3 x 16 (process-wide).
 int set_rb13(int rb);
-// How many of a phase's targets (tile bits >= 4) may sit on lane bits 3, 4 (0..2; default 2).
+// How many of a phase's targets (tile bits >= 4) may sit on lane bits 3, 4 (0..2; default 1).
 int set_phase_lanes(int k);
 // Register/warp bit split of the complex128 layout for a window of kw qubits (kw in 10..12): tile bits
 // 0-2 on lane bits 0-2, two chosen lane bits, 4 register bits, kw - 9 warp bits.

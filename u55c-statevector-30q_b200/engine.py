@@ -330,8 +330,8 @@ JIT_MODES = {"off": 0, "eager": 1, "auto": 2}
 
 def set_jit(mode):
     """Specialised sweep kernels: "off" (interpreter only), "eager" (compile each new sweep structure before
-    its first launch) or "auto" (default: compile in the background once a structure repeats). Values are
-    identical in every mode. Returns the previous mode's name."""
+    its first launch) or "auto" (default: compile in the background once a structure's launches have swept
+    2^31 amplitudes). Values are identical in every mode. Returns the previous mode's name."""
     rc = load().qsv_set_jit(JIT_MODES[mode] if isinstance(mode, str) else int(mode))
     if rc < 0:
         _check(rc)
