@@ -257,7 +257,7 @@ def served_main(a):
     count = a.count or 400
     workers = min(16, os.cpu_count() or 1)
     reqs = serve.precompile(serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax), workers=workers)
-    srv = serve.Server(budget_bytes=160e9, max_inflight=16)
+    srv = serve.Server(budget_bytes=160e9, max_inflight=16, policy=a.policy)
     with ClockSampler(0) as clk:
         t = time.perf_counter()
         done = srv.run(reqs)
@@ -275,7 +275,8 @@ def served_main(a):
                       "value": st["circuits_per_s"], "unit": "circuits/s", "higher_is_better": True,
                       "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)", "data": "synthetic (seeded requests)",
                       "config": {"workload": f"{count} Poisson arrivals at {a.rate}/s, n log-uniform in "
-                                             f"[12, {a.qmax}], depth uniform in [10, 100], 160 GB HBM budget"},
+                                             f"[12, {a.qmax}], depth uniform in [10, 100], 160 GB HBM budget",
+                                 "admission": a.policy},
                       "served": dict(st, wall_s=t_served, **srv.stats), "plain": dict(sp, wall_s=t_plain),
                       "speedup_vs_plain": st["circuits_per_s"] / sp["circuits_per_s"],
                       "results_identical_alone_and_in_mix": equal, "clocks": clk.summary()}))
@@ -303,6 +304,7 @@ def main():
     ap.add_argument("--count", type=int, default=0, help="circuits (batched: 512; served: 400)")
     ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
     ap.add_argument("--qmax", type=int, default=24, help="served: largest qubit count")
+    ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"], help="served: admission order")
     a = ap.parse_args()
     if a.workload == "precision":
         return precision_main(a)

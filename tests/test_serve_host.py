@@ -21,3 +21,27 @@ def test_config5_requests_distribution():
     assert config5_requests(count=5, seed=4)[3].spec == reqs[3].spec
     ds = np.array([r.spec[1] for r in reqs])
     assert ds.min() >= 10 and ds.max() <= 100
+
+
+def test_ready_queue_orders():
+    """Shortest estimated work first, but a request that waited longer than max_wait goes first; FIFO
+    policy keeps arrival order."""
+    from qsv_b200.serve import _ReadyQueue, Request
+
+    def drain(q, now):
+        out = []
+        while (r := q.peek(now)) is not None:
+            q.take(r)
+            out.append(r.rid)
+        return out
+
+    def fill(q):
+        for i, w in enumerate([50, 10, 30, 20, 40]):
+            r = Request(i, None, 0.1 * i)
+            r.work = w
+            q.append(r)
+        return q
+
+    assert drain(fill(_ReadyQueue("sjf", max_wait=10.0)), 0.5) == [1, 3, 2, 4, 0]
+    assert drain(fill(_ReadyQueue("sjf", max_wait=0.2)), 0.35) == [0, 1, 3, 2, 4]
+    assert drain(fill(_ReadyQueue("fifo")), 0.5) == [0, 1, 2, 3, 4]

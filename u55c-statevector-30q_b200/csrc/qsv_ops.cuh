@@ -288,9 +288,11 @@ __device__ __forceinline__ void lane_op_fast(float2 (&R)[NV], float2 (&I)[NV], c
     const int var = op.variant;
     if (var == QSV_V_UNI_DENSE || var == QSV_V_CTRL_DENSE || var == QSV_V_CTRL_DENSE_SEL) {
         const bool uni = var == QSV_V_UNI_DENSE;
-        const float *m = uni ? m0 : m1;
-        const float a_r = mine ? m[6] : m[0], a_i = mine ? m[7] : m[1];
-        const float b_r = mine ? m[4] : m[2], b_i = mine ? m[5] : m[3];
+        // value selects (a pointer select between the two coefficient arrays would put them in local memory)
+        const float a_r = uni ? (mine ? m0[6] : m0[0]) : (mine ? m1[6] : m1[0]);
+        const float a_i = uni ? (mine ? m0[7] : m0[1]) : (mine ? m1[7] : m1[1]);
+        const float b_r = uni ? (mine ? m0[4] : m0[2]) : (mine ? m1[4] : m1[2]);
+        const float b_i = uni ? (mine ? m0[5] : m0[3]) : (mine ? m1[5] : m1[3]);
         const float2 ar = f2(a_r), ai = f2(a_i), nai = f2(-a_i), br = f2(b_r), bi = f2(b_i), nbi = f2(-b_i);
         if (uni) {
 #pragma unroll

@@ -100,7 +100,9 @@ __device__ __forceinline__ void lane_op_d(double2 (&A)[NV], const QsvOpD &op, co
         oth.y = __shfl_xor_sync(0xffffffffu, A[r].y, xm);
         const bool use1 = kind != QSV_K_UNI && tok && (r & cm_reg) == cm_reg;
         if (kind == QSV_K_CTRL && !use1) continue;
-        own_apply_d(A[r], oth, use1 ? m1 : m0, use1 ? cls1 : cls0, mine);
+        // separate calls: a pointer select between the coefficient arrays would put them in local memory
+        if (use1) own_apply_d(A[r], oth, m1, cls1, mine);
+        else own_apply_d(A[r], oth, m0, cls0, mine);
     }
 }
 

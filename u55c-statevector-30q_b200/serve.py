@@ -38,6 +38,7 @@ class Request:
     done: float = None
     result: object = None
     state: object = None
+    work: int = 0                   # estimated device work: 2^n x op records of the program
 
 
 @dataclass
@@ -92,8 +93,43 @@ def _compile_request(payload):
     return [s for _, s in prog], fmap, m
 
 
+class _ReadyQueue:
+    """Requests whose program exists, waiting for admission. policy "sjf": smallest estimated work first,
+    except that a request waiting longer than max_wait seconds goes first (no starvation); "fifo": arrival
+    order. Admitted requests are dropped lazily from both orders."""
+
+    def __init__(self, policy="sjf", max_wait=10.0):
+        self.policy, self.max_wait = policy, max_wait
+        self.fifo = deque()          # arrival order
+        self.heap = []               # (work, sequence, request)
+        self.seq = 0
+        self.taken = set()           # sequence numbers of admitted requests
+
+    def append(self, r):
+        r._seq = self.seq
+        self.fifo.append(r)
+        heapq.heappush(self.heap, (r.work, self.seq, r))
+        self.seq += 1
+
+    def peek(self, now):
+        while self.fifo and self.fifo[0]._seq in self.taken:
+            self.fifo.popleft()
+        while self.heap and self.heap[0][1] in self.taken:
+            heapq.heappop(self.heap)
+        if not self.fifo:
+            return None
+        oldest = self.fifo[0]
+        if self.policy == "fifo" or now - oldest.arrival > self.max_wait:
+            return oldest
+        return self.heap[0][2]
+
+    def take(self, r):
+        self.taken.add(r._seq)
+
+
 class Server:
-    def __init__(self, budget_bytes=160e9, max_inflight=16, device=None, k=12, compile_workers=0):
+    def __init__(self, budget_bytes=160e9, max_inflight=16, device=None, k=12, compile_workers=0, policy="sjf",
+                 max_wait=10.0):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("Server needs a CUDA device (B200); none is available")
@@ -105,6 +141,7 @@ class Server:
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max_inflight)]
         self.free_streams = deque(range(max_inflight))
         self.used = 0
+        self.policy, self.max_wait = policy, max_wait
         self.stats = dict(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0)
         self.pool = None
         if compile_workers:
@@ -129,6 +166,7 @@ class Server:
     @staticmethod
     def _finish_compile(req, res):
         req.program, req.fmap, req.n = res
+        req.work = (1 << req.n) * sum(len(seg) for seg in req.program)
         _circuit(req)
 
     def _launch(self, reqs, now):
@@ -175,11 +213,11 @@ class Server:
         import torch
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         compiling = deque()
-        ready = deque()
+        ready = _ReadyQueue(self.policy, self.max_wait)
         inflight = []
         done = []
         t0 = time.perf_counter()
-        while pending or compiling or ready or inflight:
+        while pending or compiling or ready.peek(time.perf_counter() - t0) is not None or inflight:
             now = time.perf_counter() - t0
             if now > timeout:
                 raise TimeoutError("serving run exceeded its time limit")
@@ -204,14 +242,16 @@ class Server:
             admit = []
             streams_left = len(self.free_streams)
             small_group = False
-            while ready and streams_left > 0:
-                r = ready[0]
+            while streams_left > 0:
+                r = ready.peek(now)
+                if r is None:
+                    break
                 fp = self.footprint(r.n)
                 if self.used + fp > self.budget:
                     if not inflight and not admit:
                         raise MemoryError(f"request {r.rid} ({r.n} qubits) exceeds the HBM budget")
                     break
-                ready.popleft()
+                ready.take(r)
                 self.used += fp
                 admit.append(r)
                 if r.n <= SMALL_MAX:
@@ -252,7 +292,7 @@ class Server:
             if not admit and not finished_streams:
                 # nothing to do right now: wait for the next arrival, compile or completion
                 wait = 0.0005
-                if pending and realtime and not ready and not inflight and not compiling:
+                if pending and realtime and ready.peek(now) is None and not inflight and not compiling:
                     wait = max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0)))
                 time.sleep(wait)
         return done
