@@ -136,7 +136,7 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
     for (int o = 0; o < sw.nops; o++) {
         const QsvOp &op = sw.ops[o];
         put(op.slot); put(op.variant); put(op.cm_reg); put32(op.cm_thr);
-        put(op.kind); put(op.cls0); put(op.cls1); put(op.cm_c);
+        put(op.kind); put(op.cls0); put(op.cls1); put(op.cm_c); put(op.r00);
     }
     return k;
 }
@@ -167,7 +167,11 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
         for (int o = ph.op_begin; o < ph.op_end; o++) {
             const QsvOp &op = sw.ops[o];
             const std::string thr = std::to_string(op.cm_thr) + "u";
-            const std::string cls = std::to_string((int)op.kind) + ", " + std::to_string((int)op.cls0) + ", " +
+            // m00-real dense ops take the QSV_M_DENSE_R0 / QSV_V_UNI_DENSE_R0 code paths
+            const bool r0 = op.r00 && op.kind == QSV_K_UNI;
+            const int cls0 = r0 ? QSV_M_DENSE_R0 : op.cls0;
+            const int var = (r0 && op.variant == QSV_V_UNI_DENSE) ? QSV_V_UNI_DENSE_R0 : op.variant;
+            const std::string cls = std::to_string((int)op.kind) + ", " + std::to_string(cls0) + ", " +
                                     std::to_string((int)op.cls1) + ", ";
             const std::string ctl = std::to_string((int)op.cm_reg) + ", " + thr;
             const std::string mux = std::to_string((int)op.kind) + ", " + std::to_string((int)op.cls1) + ", " +
@@ -178,7 +182,7 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
                 s << "            jit_reg_mux<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << mux << ">(R, I, P.ops[" << o
                   << "], tb);\n";
             else if (op.slot < QSV_SLOT_LANE0)
-                s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << (int)op.variant << ", " << ctl
+                s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb);\n";
             else if (op.variant == QSV_V_MUX)
                 s << "            jit_lane_mux<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << mux << ">(R, I, P.ops["

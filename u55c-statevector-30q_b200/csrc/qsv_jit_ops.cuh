@@ -68,6 +68,12 @@ __device__ __forceinline__ void jit_reg(float2 (&R)[NV], float2 (&I)[NV], const 
 #pragma unroll
         for (int r = 0; r < NV; r++)
             if (!(r & B)) dense2(R[r], I[r], R[r | B], I[r | B], m);
+    } else if constexpr (VAR == QSV_V_UNI_DENSE_R0) {
+        float m[8];
+        jit_mat(m, op.m0);
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            if (!(r & B)) dense2_r0(R[r], I[r], R[r | B], I[r | B], m);
     } else if constexpr (VAR == QSV_V_UNI_DIAG) {
         const float a0 = op.m0[0], a1 = op.m0[1], d0 = op.m0[6], d1 = op.m0[7];
 #pragma unroll

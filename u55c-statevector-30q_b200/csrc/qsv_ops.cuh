@@ -28,6 +28,19 @@ __device__ __forceinline__ void dense2(float2 &R0, float2 &I0, float2 &R1, float
     const float2 y1i = __ffma2_rn(f2(m[6]), I1, u);
     R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
 }
+// dense with m00 real: the two m00.im terms (exact zeros) are skipped; same values as dense2
+__device__ __forceinline__ void dense2_r0(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float *m) {
+    float2 t, u;
+    t = __fmul2_rn(f2(-m[3]), I1); t = __ffma2_rn(f2(m[2]), R1, t);
+    const float2 y0r = __ffma2_rn(f2(m[0]), R0, t);
+    u = __fmul2_rn(f2(m[3]), R1);  u = __ffma2_rn(f2(m[2]), I1, u);
+    const float2 y0i = __ffma2_rn(f2(m[0]), I0, u);
+    t = __fmul2_rn(f2(-m[5]), I0); t = __ffma2_rn(f2(m[4]), R0, t); t = __ffma2_rn(f2(-m[7]), I1, t);
+    const float2 y1r = __ffma2_rn(f2(m[6]), R1, t);
+    u = __fmul2_rn(f2(m[5]), R0);  u = __ffma2_rn(f2(m[4]), I0, u); u = __ffma2_rn(f2(m[7]), R1, u);
+    const float2 y1i = __ffma2_rn(f2(m[6]), I1, u);
+    R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
+}
 // dense with per-lane coefficients (c[e] = (coefficient for pair .x, coefficient for pair .y))
 __device__ __forceinline__ void dense2v(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float2 *c) {
     const float2 n1 = make_float2(-c[1].x, -c[1].y), n3 = make_float2(-c[3].x, -c[3].y);
@@ -64,8 +77,13 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
 #define QSV_P1 (r | (1 << RBIT))
     switch (op.variant) {
         case QSV_V_UNI_DENSE:
+            if (op.r00) {
 #pragma unroll
-            QSV_FOR_PAIRS dense2(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+                QSV_FOR_PAIRS dense2_r0(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+            } else {
+#pragma unroll
+                QSV_FOR_PAIRS dense2(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+            }
             break;
         case QSV_V_UNI_DIAG:
 #pragma unroll
@@ -222,6 +240,13 @@ __device__ __forceinline__ void pair_t(float &x0r, float &x0i, float &x1r, float
         lin_own(y0r, y0i, m[0], m[1], m[2], m[3], x0r, x0i, x1r, x1i);
         lin_own(y1r, y1i, m[6], m[7], m[4], m[5], x1r, x1i, x0r, x0i);
         x0r = y0r; x0i = y0i; x1r = y1r; x1i = y1i;
+    } else if constexpr (CLS == QSV_M_DENSE_R0) {
+        // m00.im is an exact zero: its two terms are skipped
+        const float t = fmaf(m[2], x1r, -__fmul_rn(m[3], x1i));
+        const float u = fmaf(m[2], x1i, __fmul_rn(m[3], x1r));
+        float y1r, y1i;
+        lin_own(y1r, y1i, m[6], m[7], m[4], m[5], x1r, x1i, x0r, x0i);
+        x0r = fmaf(m[0], x0r, t); x0i = fmaf(m[0], x0i, u); x1r = y1r; x1i = y1i;
     } else if constexpr (CLS == QSV_M_DIAG) {
         float y0r, y0i, y1r, y1i;
         diag_own(y0r, y0i, m[0], m[1], x0r, x0i);
@@ -259,7 +284,10 @@ __device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], c
     const int cm_reg = op.cm_reg;
     if (op.kind == QSV_K_UNI) {
         switch (op.cls0) {
-            case QSV_M_DENSE: comp_loop<NV, QSV_M_DENSE, false>(R, I, m0, 0, true); return;
+            case QSV_M_DENSE:
+                if (op.r00) comp_loop<NV, QSV_M_DENSE_R0, false>(R, I, m0, 0, true);
+                else comp_loop<NV, QSV_M_DENSE, false>(R, I, m0, 0, true);
+                return;
             case QSV_M_DIAG: comp_loop<NV, QSV_M_DIAG, false>(R, I, m0, 0, true); return;
             case QSV_M_DIAG1: comp_loop<NV, QSV_M_DIAG1, false>(R, I, m0, 0, true); return;
             case QSV_M_XSWAP: comp_loop<NV, QSV_M_XSWAP, false>(R, I, m0, 0, true); return;

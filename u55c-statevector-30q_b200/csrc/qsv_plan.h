@@ -53,6 +53,9 @@ typedef unsigned long long uint64_t;
 #define QSV_M_IDENT 2           // identity: pair left unchanged
 #define QSV_M_XSWAP 3           // [[0,1],[1,0]]: the two amplitudes are exchanged
 #define QSV_M_DIAG1 4           // diag(1, d): only the bit-1 amplitude changes
+// dense with m00 real (its imaginary part an exact zero, as in every U3): the two m00.im terms of the
+// chain are skipped. Used as a code path only; op records keep QSV_M_DENSE and set r00.
+#define QSV_M_DENSE_R0 5
 
 // op kinds
 #define QSV_K_UNI 0             // one matrix (M0) for every pair
@@ -72,6 +75,8 @@ typedef unsigned long long uint64_t;
 #define QSV_V_CTRL_DENSE_SEL 8
 #define QSV_V_CTRL_DIAG1_SEL 9
 #define QSV_V_CTRL_SWAP_SEL 10
+// code path only (op records keep QSV_V_UNI_DENSE and set r00): dense with m00 real, register-bit target
+#define QSV_V_UNI_DENSE_R0 11
 
 // where the target of an op lives in its phase
 #define QSV_SLOT_COMP 0         // tile bit 0 (inside a float4)
@@ -91,7 +96,8 @@ struct QsvOp {
     uint8_t slot;               // QSV_SLOT_*
     uint8_t tbit;               // target tile bit
     uint8_t variant;            // QSV_V_*
-    uint8_t pad[3];
+    uint8_t r00;                // 1: M0 is dense with m00 real (QSV_M_DENSE_R0 path)
+    uint8_t pad[2];
 };
 
 // complex128 op: the same fields with FP64 matrices. In the complex128 layout tile bits 0-2 are lane bits
@@ -109,7 +115,8 @@ struct QsvOpD {
     uint8_t slot;
     uint8_t tbit;
     uint8_t variant;
-    uint8_t pad[7];
+    uint8_t r00;
+    uint8_t pad[6];
 };
 
 struct QsvPhase {

@@ -217,6 +217,7 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             std::memcpy(o.m1, o.m0, sizeof(o.m0));
             o.cls1 = o.cls0;
         }
+        o.r00 = (uint8_t)(o.cls0 == QSV_M_DENSE && o.m0[1] == 0);
         if (o.cmask == 0) { o.kind = QSV_K_UNI; o.cls = o.cls0; }
         else if (o.cls0 == QSV_M_IDENT) { o.kind = QSV_K_CTRL; o.cls = o.cls1; }
         else { o.kind = QSV_K_MUX; o.cls = QSV_M_DENSE; }
