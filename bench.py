@@ -289,7 +289,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--n", "--qubits", dest="n", type=int, default=30)
     ap.add_argument("--depth", type=int, default=24)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -1,0 +1,105 @@
+"""Full-size checks (30 and 33 qubits) through size-independent properties, where the oracle cannot run:
+* QFT-30 from |0...0>: every amplitude is 2^-15 (uniform superposition; the reference's analytic check,
+  tests/functional_suite.py:74-82) -- checked on the device through the FP64 reductions and samples;
+* GHZ-30: amplitudes 0 and 2^30 - 1 are 1/sqrt(2), everything else is zero;
+* random-layer 30q depth 24 (the benchmark circuit) and the 33-qubit complex64 state: the norm stays 1
+  (1e-4) and the specialised kernels give the interpreter's state bit for bit;
+* a remap at 30 qubits followed by its inverse restores the state exactly."""
+import numpy as np
+import pytest
+
+import qsv_b200 as q
+from qsv_b200 import engine, generators as gen
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    engine.load()
+    return t
+
+
+def _run(torch, qc, n, jit="auto", dtype="c64"):
+    old = engine.set_jit(jit)
+    try:
+        prog, fmap, _ = q.compile_circuit(qc, n, 12, dtype=dtype)
+        st = engine.new_state(n, dtype=dtype)
+        alt = None
+        for kind, payload in prog:
+            if kind == "segment":
+                engine.run_segment(st, payload)
+            else:
+                alt = torch.empty_like(st) if alt is None else alt
+                engine.remap(st, alt, payload)
+                st, alt = alt, st
+        torch.cuda.synchronize()
+        assert engine.device_status() == 0
+        return st, fmap
+    finally:
+        engine.set_jit(old)
+
+
+@pytest.mark.timeout(900)
+def test_qft30_uniform(torch):
+    n = 30
+    st, fmap = _run(torch, gen.qft(n), n, jit="eager")
+    z = engine.reduce_f64(st).cpu().numpy()
+    assert abs(z[0] - 1) < 1e-5 and np.max(np.abs(z[1:])) < 1e-5
+    a = torch.abs(st)
+    lo, hi = float(a.min()), float(a.max())
+    assert abs(lo - 2 ** -15) < 1e-9 and abs(hi - 2 ** -15) < 1e-9
+    del st, a
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.timeout(900)
+def test_ghz30(torch):
+    n = 30
+    st, fmap = _run(torch, gen.ghz(n), n)
+    s = 1 / np.sqrt(2)
+    ends = st[[0, (1 << n) - 1]].cpu().numpy()
+    assert np.allclose(np.abs(ends), s, atol=1e-6)
+    z = engine.reduce_f64(st).cpu().numpy()
+    assert abs(z[0] - 1) < 1e-6 and np.max(np.abs(z[1:])) < 1e-6
+    del st
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("n,depth,circ", [(30, 24, "random_layer"), (33, 4, "random_layer_ccx")])
+def test_norm_and_specialised_equal_interpreter(torch, n, depth, circ):
+    qc = getattr(gen, circ)(n, depth, 1)
+    a, _ = _run(torch, qc, n, jit="eager")
+    za = engine.reduce_f64(a).cpu().numpy()
+    assert abs(za[0] - 1) < 1e-4
+    if n <= 30:            # two 30-qubit states fit side by side; at 33 qubits one state is 64 GiB
+        b, _ = _run(torch, qc, n, jit="off")
+        assert torch.equal(a, b)
+        del b
+    del a
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.timeout(900)
+def test_remap30_roundtrip(torch):
+    n = 30
+    st, _ = _run(torch, gen.random_layer(n, 2, 4), n)
+    perm = [int(x) for x in np.random.default_rng(5).permutation(n)]
+    inv = [0] * n
+    for j, p in enumerate(perm):
+        inv[p] = j
+    dst = torch.empty_like(st)
+    engine.remap(st, dst, perm)
+    back = torch.empty_like(st)
+    engine.remap(dst, back, inv)
+    assert torch.equal(back, st)
+    # one amplitude moved as the permutation says: dst[y] = st[x], bit j of y = bit perm[j] of x
+    x = 0x2A5A5A5A & ((1 << n) - 1)
+    y = sum(((x >> perm[j]) & 1) << j for j in range(n))
+    assert complex(dst[y].item()) == complex(st[x].item())
+    del st, dst, back
+    torch.cuda.empty_cache()
