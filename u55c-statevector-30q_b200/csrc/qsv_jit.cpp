@@ -50,15 +50,27 @@ constexpr size_t kMaxQueued = 64;
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
 
-// consumer groups per CTA. One by default; QSV_JIT_GROUPS13=2 gives 13-qubit windows with 8-warp groups
-// two groups taking alternate tiles (16 consumer warps, registers capped near 96 per thread). Measured on
-// the 30-qubit random-layer and QFT programs, two groups were no faster than one.
-int groups_for(int kw, int wb) {
-    static const int g13 = [] {
+// Consumer groups per CTA for a sweep. Two groups (16 consumer warps taking alternate tiles, registers
+// capped near 96 per thread) hide the phase round trips of light 13-qubit sweeps; sweeps with many dense
+// or warp-shuffle ops are FP32-bound and run faster with one group and more registers (measured on the
+// 30-qubit random-layer program: 3.05 -> 2.96 ms for 7-8 dense ops, 4.4 -> 5.3 ms for 12).
+// QSV_JIT_GROUPS13=1 or 2 forces one choice.
+int groups_for(const QsvSweep &sw, int wb) {
+    static const int forced = [] {
         const char *e = std::getenv("QSV_JIT_GROUPS13");
-        return e && std::atoi(e) == 2 ? 2 : 1;
+        return e ? std::atoi(e) : 0;
     }();
-    return kw == 13 && wb <= 3 ? g13 : 1;
+    if (sw.kw != 13 || wb > 3) return 1;
+    if (forced == 1 || forced == 2) return forced;
+    int dense = 0, lane = 0;
+    for (int o = 0; o < sw.nops; o++) {
+        const QsvOp &op = sw.ops[o];
+        const int v = op.variant;
+        dense += v == QSV_V_UNI_DENSE || v == QSV_V_CTRL_DENSE || v == QSV_V_CTRL_DENSE_SEL ||
+                 (v == QSV_V_MUX && op.cls1 == QSV_M_DENSE) || op.slot == QSV_SLOT_COMP;
+        lane += op.slot >= QSV_SLOT_LANE0 && v != QSV_V_SKIP;
+    }
+    return dense <= 8 && lane <= 2 ? 2 : 1;
 }
 
 struct Drv {
@@ -91,7 +103,7 @@ const Drv &drv() {
 enum State { kNew, kQueued, kReady, kFailed };
 
 struct Entry {
-    int kw = 0, rb = 0, wb = 0;
+    int kw = 0, rb = 0, wb = 0, groups = 1;
     std::string src;
     State state = kNew;
     std::vector<char> cubin;
@@ -143,7 +155,7 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
 
 // CUDA source of the kernel specialised to sw's structure
 std::string gen_source(const QsvSweep &sw, int rb, int wb) {
-    const int groups = groups_for(sw.kw, wb);
+    const int groups = groups_for(sw, wb);
     const int nc = 1 << (5 + wb), nt = groups * nc + 32, minb = sw.kw >= 13 ? 1 : 2;
     std::ostringstream s;
     s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
@@ -325,6 +337,7 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
     e->kw = sw.kw;
     e->rb = rb;
     e->wb = wb;
+    e->groups = groups_for(sw, wb);
     j.map.emplace(key, e);
     return e;
 }
@@ -412,7 +425,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
-    const int NT = groups_for(sw.kw, wb) * (1 << (5 + wb)) + 32;
+    const int NT = e->groups * (1 << (5 + wb)) + 32;
     const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2);
     if (!e->fn[dev]) {
         // loading a module is not a stream operation: keep it out of stream captures
