@@ -400,6 +400,33 @@ def main():
     peak, peak_kind = _peaks()
     achieved = bytes_per_sweep / per_launch / 1e9
 
+    # config 2's second circuit, QFT-30 (H, controlled phases, reversal swaps), timed the same way; reported
+    # beside the headline, which stays the random-layer circuit
+    qft = None
+    if a.n == 30 and world == 1:
+        qprog, _, qstats = pkg.compile_circuit(pkg.generators.qft(a.n), a.n, 12)
+        qsegs = [p for kind, p in qprog if kind == "segment"]
+        if a.jit != "off":
+            for s_ in qsegs:
+                engine.jit_prepare(s_, a.n)
+        qsweeps = sum(len(engine.plan_segment(s_, a.n)) for s_ in qsegs)
+        for _ in range(2):
+            for s_ in qsegs:
+                engine.run_segment(state, s_, stream)
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(3):
+            for s_ in qsegs:
+                engine.run_segment(state, s_, stream)
+        q1.record(stream)
+        torch.cuda.synchronize(dev)
+        qsec = q0.elapsed_time(q1) / 1e3 / 3
+        qgbs = bytes_per_sweep * qsweeps / qsec / 1e9
+        qft = {"workload": "qft n=30 (H, CP, reversal swaps as relabels)", "sweeps": qsweeps,
+               "qsv2_passes": qstats.n_passes, "ms_per_step": qsec * 1e3, "value": qgbs, "unit": "GB/s",
+               "frac": qgbs / _peaks()[0]}
+
     # end to end through the public API (host circuit in, sampled counts out)
     e2e = None
     if a.e2e_steps > 0:
@@ -439,7 +466,7 @@ def main():
                                        else "qsv::dev::sweep_kernel<13,4,3,3>" if jit_launches == 0
                                        else f"qsv_sweep_jit x{jit_launches} + sweep_kernel x{launches - jit_launches}"),
                             "algorithmic_bytes_per_launch": bytes_per_sweep},
-               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "qft30": qft,
                # the reference's own formula (analysis/make_tables.py:321): QSV2 passes x 16 B x 2^n over
                # the kernel time; above the HBM roofline because consecutive passes share one sweep here
                "reference_formula_gbs": stats.n_passes * bytes_per_sweep * a.steps * world / sec / 1e9}

@@ -90,3 +90,30 @@ def test_batch_runner_matches_fp64_and_is_packing_independent(torch):
         alone = runner.prepare([circs[i]], sample_fraction=0)
         za, _ = runner.run(alone)
         assert za[0][0] == z[i][0] and np.array_equal(za[0][1], z[i][1])
+
+
+def test_graph_capture_with_specialised_kernels(torch):
+    """Sweeps whose specialised kernels are compiled and loaded before the capture are launched through
+    the driver API inside the CUDA-graph capture; replays equal the interpreter-only plain path."""
+    from qsv_b200.batch import plain_run, compile_many
+    circs = [gen.random_layer(n, 6, 300 + n) for n in (14, 16, 18, 20)] + [gen.random_layer(16, 6, 316)]
+    progs = compile_many(circs)
+    old = engine.set_jit("eager")
+    try:
+        runner = BatchRunner(streams=3, autotune=False)
+        plan = runner.prepare(circs, sample_fraction=0.0, programs=progs)
+        before = engine.jit_info()["jit_launches"]
+        runner.capture(plan)          # eager pass (compiles + loads), then the capture
+        z1, _ = runner.run(plan)
+        z2, _ = runner.run(plan)
+        assert engine.jit_info()["jit_launches"] > before
+    finally:
+        engine.set_jit(old)
+    engine.set_jit("off")
+    try:
+        zp = plain_run(circs, progs)
+    finally:
+        engine.set_jit(old)
+    assert engine.device_status() == 0
+    for a, b, c in zip(z1, z2, zp):
+        assert a[0] == b[0] == c[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[1], c[1])
