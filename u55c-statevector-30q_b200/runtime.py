@@ -108,6 +108,9 @@ class SVRuntime:
     def run(self, qc, shots=1024, k=KMAX, p_max=None, fuse=True, tiling=True, initial_map=None,
             return_state=True, seed=None):
         import torch
+        if isinstance(qc, str):          # OpenQASM 2 text or a .qasm path (the reference's circuit files)
+            from .qasm import from_qasm
+            qc = from_qasm(qc)
         n = qc.num_qubits
         P, n_run, L = self.plan(n, p_max)
         k = min(k, L)
