@@ -68,10 +68,16 @@ class Circuit:
         return method
 
     def mcx(self, controls, target):
-        return self.append("mcx", tuple(controls) + (target,))
+        controls = tuple(controls)
+        if len(controls) == 1:          # as Qiskit's mcx: one control is a CX
+            return self.append("cx", controls + (target,))
+        return self.append("mcx", controls + (target,))
 
     def mcp(self, lam, controls, target):
-        return self.append("mcp", tuple(controls) + (target,), (lam,))
+        controls = tuple(controls)
+        if len(controls) == 1:
+            return self.append("cp", controls + (target,), (lam,))
+        return self.append("mcp", controls + (target,), (lam,))
 
     def barrier(self, *qs):
         return self.append("barrier", qs or range(self.num_qubits))
