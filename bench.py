@@ -243,7 +243,8 @@ def served_main(a):
     """Served: Poisson arrivals (rate per second) of circuits with qubit counts log-uniform in [12, qmax]
     and depths uniform in [10, 100] (U3 / CZ / Toffoli layers, request i seeded 4 + i), admitted under a
     160 GB HBM budget with continuous batching, against the plain sequential path on the same requests.
-    Programs are compiled before the run (spawned workers), so both sides time device work and queueing."""
+    Programs are compiled before the run (spawned workers), so both sides time device work and queueing;
+    --compile-on-arrival compiles in a worker pool as requests arrive (the plain path compiles in line)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     pkg = _package()
@@ -256,15 +257,20 @@ def served_main(a):
     engine.set_jit(a.jit)
     count = a.count or 400
     workers = min(16, os.cpu_count() or 1)
-    reqs = serve.precompile(serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax), workers=workers)
-    srv = serve.Server(budget_bytes=160e9, max_inflight=16, policy=a.policy)
+    reqs = serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax)
+    if not a.compile_on_arrival:
+        reqs = serve.precompile(reqs, workers=workers)
+    srv = serve.Server(budget_bytes=160e9, max_inflight=16, policy=a.policy,
+                       compile_workers=workers if a.compile_on_arrival else 0)
     with ClockSampler(0) as clk:
         t = time.perf_counter()
         done = srv.run(reqs)
         t_served = time.perf_counter() - t
     srv.close()
     st = serve.latency_stats(done)
-    reqs2 = serve.precompile(serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax), workers=workers)
+    reqs2 = serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax)
+    if not a.compile_on_arrival:
+        reqs2 = serve.precompile(reqs2, workers=workers)
     t = time.perf_counter()
     plain = serve.plain_serve(reqs2)
     t_plain = time.perf_counter() - t
@@ -276,7 +282,9 @@ def served_main(a):
                       "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)", "data": "synthetic (seeded requests)",
                       "config": {"workload": f"{count} Poisson arrivals at {a.rate}/s, n log-uniform in "
                                              f"[12, {a.qmax}], depth uniform in [10, 100], 160 GB HBM budget",
-                                 "admission": a.policy},
+                                 "admission": a.policy,
+                                 "compile": "on arrival (worker pool; plain path in line)" if a.compile_on_arrival
+                                 else "before the run"},
                       "served": dict(st, wall_s=t_served, **srv.stats), "plain": dict(sp, wall_s=t_plain),
                       "speedup_vs_plain": st["circuits_per_s"] / sp["circuits_per_s"],
                       "results_identical_alone_and_in_mix": equal, "clocks": clk.summary()}))
@@ -305,6 +313,9 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
     ap.add_argument("--qmax", type=int, default=24, help="served: largest qubit count")
     ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"], help="served: admission order")
+    ap.add_argument("--compile-on-arrival", action="store_true",
+                    help="served: compile each request when it arrives (spawned worker pool) instead of before "
+                         "the run; the plain path then compiles in line as well")
     a = ap.parse_args()
     if a.workload == "precision":
         return precision_main(a)
