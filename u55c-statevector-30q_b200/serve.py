@@ -33,7 +33,8 @@ class Request:
     # filled in by the server
     program: object = None
     fmap: list = None
-    n: int = 0
+    n: int = 0                      # qubits the program runs on (at least the engine's minimum)
+    n_log: int = 0                  # qubits of the request's circuit
     admitted: float = None
     done: float = None
     result: object = None
@@ -76,7 +77,7 @@ def _circuit(req):
 
 
 def _compile_request(payload):
-    """Compile one request (runs in a worker process or inline): -> (segments, final_map, n_run)."""
+    """Compile one request (runs in a worker process or inline): -> (segments, final_map, n_run, n)."""
     circuit, spec, k = payload
     req = Request(-1, circuit, 0.0, spec=spec)
     qc = _circuit(req)
@@ -90,7 +91,7 @@ def _compile_request(payload):
     prog, fmap, _ = compile_circuit(qc, m, m if m <= SMALL_MAX else k)
     if any(kind != "segment" for kind, _ in prog):
         raise ValueError("program needs remaps, not served here")
-    return [s for _, s in prog], fmap, m
+    return [s for _, s in prog], fmap, m, n
 
 
 class _ReadyQueue:
@@ -165,9 +166,9 @@ class Server:
 
     @staticmethod
     def _finish_compile(req, res):
-        req.program, req.fmap, req.n = res
+        # the circuit itself stays where it was built (a worker process): only its program comes back
+        req.program, req.fmap, req.n, req.n_log = res
         req.work = (1 << req.n) * sum(len(seg) for seg in req.program)
-        _circuit(req)
 
     def _launch(self, reqs, now):
         """Start a group of admitted requests: small ones as one whole-circuit batch, large ones alone."""
@@ -273,7 +274,7 @@ class Server:
                     z = sl.zout.cpu().numpy()
                     r = sl.req
                     r.done = time.perf_counter() - t0
-                    n_log = r.circuit.num_qubits
+                    n_log = r.n_log
                     r.result = (float(z[0]), np.array([z[1 + r.fmap[q]] for q in range(n_log)]))
                     if r.want_state:
                         perm = [r.fmap[q] for q in range(r.n)]
@@ -341,7 +342,7 @@ def plain_serve(requests, device=None):
                 engine.run_segment(st, seg)
         z = engine.reduce_f64(st).cpu().numpy()
         r.done = time.perf_counter() - t0
-        n_log = r.circuit.num_qubits
+        n_log = r.n_log
         r.result = (float(z[0]), np.array([z[1 + r.fmap[q]] for q in range(n_log)]))
         out.append(r)
         del st
