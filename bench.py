@@ -309,6 +309,46 @@ def served_main(a):
                       "results_identical_alone_and_in_mix": equal, "clocks": clk.summary()}))
 
 
+def latency_main(a):
+    """Latency distribution of repeated small circuits through the public API, the reference's determinism
+    study (bench/latency_jitter.py:16-63): each family and size run 20 warm-up + `count` (default 2000)
+    times with SVRuntime.run(qc, shots=1024, return_state=False); p50 / p99 / max of T_e2e and T_kernel."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    pkg = _package()
+    import torch
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    runtime = import_module("qsv_b200.runtime")
+    engine.load()
+    torch.cuda.set_device(0)
+    runs = a.count or 2000
+    rt = runtime.SVRuntime()
+    out = []
+    for fam in ("ghz", "rqc"):
+        for n in (4, 8, 12, 16):
+            qc = getattr(pkg.generators, fam)(n)
+            e2e, ker = [], []
+            for i in range(runs + 20):
+                r = rt.run(qc, shots=1024, return_state=False, seed=i)
+                e2e.append(r["timing"]["T_e2e"])
+                ker.append(r["timing"]["T_kernel"])
+            x, k = np.array(e2e[20:]) * 1e3, np.array(ker[20:]) * 1e3
+            out.append({"circuit": qc.name, "n": n, "runs": runs, "e2e_p50_ms": float(np.percentile(x, 50)),
+                        "e2e_p99_ms": float(np.percentile(x, 99)), "e2e_max_ms": float(x.max()),
+                        "kernel_p50_ms": float(np.percentile(k, 50)), "kernel_p99_ms": float(np.percentile(k, 99))})
+    ref = {"rqc_16_d10": (32.4, 36.9), "ghz_16": (5.89, 9.15)}     # U55C, results/processed/jitter_summary.csv
+    for o in out:
+        if o["circuit"] in ref:
+            o["reference_u55c_p50_p99_ms"] = ref[o["circuit"]]
+    r16 = next(o for o in out if o["circuit"] == "rqc_16_d10")
+    print(json.dumps({"metric": "T_e2e latency p50 / p99 of repeated circuits (SVRuntime.run, 1024 shots)",
+                      "value": r16["e2e_p99_ms"], "unit": "ms (p99, rqc_16_d10)", "higher_is_better": False,
+                      "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)", "data": "synthetic (seeded circuits)",
+                      "config": {"workload": f"ghz and rqc (depth 10) at 4, 8, 12, 16 qubits, {runs} runs each after "
+                                             "20 warm-up runs"}, "circuits": out}))
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -323,7 +363,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
                     help="specialised sweep kernels (compiled before the warm-up unless off)")
-    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served"],
+    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served", "latency"],
                     help="rl30: the headline sweep benchmark; precision: the complex64 / complex128 study "
                          "(33 qubits complex64, 32 qubits complex128 vs complex64); batched: 512 circuits of "
                          "10..24 qubits per CUDA-graph replay vs one at a time; served: Poisson arrivals of "
@@ -342,6 +382,8 @@ def main():
         return batched_main(a)
     if a.workload == "served":
         return served_main(a)
+    if a.workload == "latency":
+        return latency_main(a)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
