@@ -349,6 +349,55 @@ def latency_main(a):
                                              "20 warm-up runs"}, "circuits": out}))
 
 
+def families_main(a):
+    """The reference's 30-qubit families (GHZ, QFT, RQC depth 10, VQE 2 layers) through SVRuntime.run
+    (1024 shots, no state read-back), beside its published U55C and A100 figures. Cold = first run in the
+    process (specialised kernels not compiled yet: interpreter, compilation queued in the background);
+    warm = median of 3 runs after the compilations finished. pass_gbs is the reference's formula
+    (QSV2 passes x 16 B x 2^30 / T_kernel, analysis/make_tables.py:321); sweep_gbs counts the sweeps run."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    pkg = _package()
+    import torch
+    from importlib import import_module
+    engine = import_module("qsv_b200.engine")
+    runtime = import_module("qsv_b200.runtime")
+    engine.load()
+    torch.cuda.set_device(0)
+    n = a.n
+    rt = runtime.SVRuntime()
+    # U55C pass GB/s and T_e2e (s), A100 Aer fp32 + cuStateVec T_e2e (s): paper/generated/macros.tex
+    ref = {"ghz": (141, 4.1, 7.16), "qft": (102, 24.5, 7.29), "rqc": (67, 20.7, 7.24), "vqe": (80, None, 7.28)}
+    out = []
+    for fam in ("ghz", "qft", "rqc", "vqe"):
+        qc = getattr(pkg.generators, fam)(n)
+        t0 = time.perf_counter()
+        cold = rt.run(qc, shots=1024, return_state=False, seed=0)
+        cold_s = time.perf_counter() - t0
+        engine.jit_wait()
+        warm = []
+        for i in range(3):
+            warm.append(rt.run(qc, shots=1024, return_state=False, seed=1 + i))
+        w = sorted(warm, key=lambda r: r["timing"]["T_e2e"])[1]
+        tk = w["timing"]["T_kernel"]
+        passes = w["stats"]["n_passes"]
+        prog, _, _ = pkg.compile_circuit(qc, n, 12)
+        sweeps = sum(len(engine.plan_segment(s_, n)) for k_, s_ in prog if k_ == "segment")
+        rec = {"circuit": qc.name, "passes": passes, "sweeps": sweeps, "ops": w["stats"]["n_ops"],
+               "cold_e2e_s": cold_s, "T_compile_s": w["timing"]["T_compile"], "T_kernel_s": tk,
+               "T_exchange_s": w["timing"]["T_exchange"], "T_e2e_s": w["timing"]["T_e2e"],
+               "pass_gbs": passes * (16 << n) / tk / 1e9, "sweep_gbs": sweeps * (16 << n) / tk / 1e9}
+        if n == 30:
+            rec["reference"] = {"u55c_pass_gbs": ref[fam][0], "u55c_T_e2e_s": ref[fam][1],
+                                "a100_aer_cusv_T_e2e_s": ref[fam][2]}
+        out.append(rec)
+    print(json.dumps({"metric": f"{n}-qubit families through SVRuntime.run (1024 shots)",
+                      "value": statistics.median(o["sweep_gbs"] for o in out), "unit": "GB/s (median sweep_gbs)",
+                      "higher_is_better": True, "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)",
+                      "data": "synthetic (seeded circuits)", "config": {"workload": f"ghz, qft, rqc d10, vqe L2 at n={n}"},
+                      "peak_gbs": _peaks()[0], "circuits": out}))
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -363,7 +412,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
                     help="specialised sweep kernels (compiled before the warm-up unless off)")
-    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served", "latency"],
+    ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served", "latency", "families"],
                     help="rl30: the headline sweep benchmark; precision: the complex64 / complex128 study "
                          "(33 qubits complex64, 32 qubits complex128 vs complex64); batched: 512 circuits of "
                          "10..24 qubits per CUDA-graph replay vs one at a time; served: Poisson arrivals of "
@@ -384,6 +433,8 @@ def main():
         return served_main(a)
     if a.workload == "latency":
         return latency_main(a)
+    if a.workload == "families":
+        return families_main(a)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
