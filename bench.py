@@ -550,6 +550,23 @@ def main():
                "qsv2_passes": qstats.n_passes, "ms_per_step": qsec * 1e3, "value": qgbs, "unit": "GB/s",
                "frac": qgbs / _peaks()[0]}
 
+    # live copy-bandwidth probe (the hand-written HBM copy kernel) on the state's size: the achievable
+    # ceiling measured in the same process, beside the driver-measured peak used for frac
+    copy_gbs = None
+    if world == 1:
+        dst = torch.empty_like(state)
+        for _ in range(2):
+            engine.hbm_copy(dst, state, stream)
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(5):
+            engine.hbm_copy(dst, state, stream)
+        c1.record(stream)
+        torch.cuda.synchronize(dev)
+        copy_gbs = 2 * (8 << a.n) * 5 / (c0.elapsed_time(c1) / 1e3) / 1e9
+        del dst
+
     # end to end through the public API (host circuit in, sampled counts out)
     e2e = None
     if a.e2e_steps > 0:
@@ -588,7 +605,8 @@ def main():
                             "kernel": ("qsv_sweep_jit (specialised per sweep structure)" if jit_launches == launches
                                        else "qsv::dev::sweep_kernel<13,4,3,3>" if jit_launches == 0
                                        else f"qsv_sweep_jit x{jit_launches} + sweep_kernel x{launches - jit_launches}"),
-                            "algorithmic_bytes_per_launch": bytes_per_sweep},
+                            "algorithmic_bytes_per_launch": bytes_per_sweep,
+                            "copy_probe_gbs": copy_gbs},
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "qft30": qft,
                # the reference's own formula (analysis/make_tables.py:321): QSV2 passes x 16 B x 2^n over
                # the kernel time; above the HBM roofline because consecutive passes share one sweep here

@@ -129,6 +129,12 @@ QSV_API int qsv_batch_launch(qsv_batch *batch, void *workspace, size_t bytes, vo
  * the number of words of the full plan, or a negative error code. Pure host code, no device work. */
 QSV_API int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap);
 
+/* HBM copy probe: dst <- src, `bytes` (a multiple of 16, 16-byte aligned, not overlapping), a grid-stride
+ * 16-byte copy that reads and writes every byte once. The measured achievable-bandwidth denominator for the
+ * sweep roofline; the B200 counterpart of the reference's FPGA HBM stream microbenchmark
+ * (kernels/hbm_stream/hbm1.cpp:38-60). Asynchronous on `stream`. */
+QSV_API int qsv_hbm_copy(void *dst, const void *src, size_t bytes, void *stream);
+
 /* Read and clear the device status word that kernels set when a bounded wait gives up (0 = clean).
  * Synchronous. */
 QSV_API int qsv_device_status(int *status);

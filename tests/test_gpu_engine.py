@@ -242,3 +242,16 @@ def test_layout13_variants_exact(torch, rb):
                     x = orc.remap(x, seg)
     finally:
         engine.set_layout13(4)
+
+
+def test_hbm_copy_probe(torch):
+    """The copy-bandwidth probe copies exactly and rejects overlapping or misaligned buffers."""
+    x = torch.from_numpy(_rand_state(20, 4)).cuda()
+    y = torch.empty_like(x)
+    engine.hbm_copy(y, x)
+    torch.cuda.synchronize()
+    assert torch.equal(x, y)
+    L = engine.load()
+    P = engine.ctypes.c_void_p
+    assert L.qsv_hbm_copy(P(x.data_ptr() + 64), P(x.data_ptr()), 1024, None) == -1
+    assert L.qsv_hbm_copy(P(y.data_ptr() + 8), P(x.data_ptr()), 1024, None) == -1

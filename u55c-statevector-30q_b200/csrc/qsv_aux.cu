@@ -83,6 +83,24 @@ __global__ void __launch_bounds__(REMAP_THREADS)
     }
 }
 
+// ---------------------------------------------------------------- HBM copy probe
+// The achievable-bandwidth denominator (the B200 counterpart of the reference's FPGA HBM stream
+// microbenchmark, kernels/hbm_stream/): a grid-stride 16-byte copy, every byte read once and written once.
+__global__ void __launch_bounds__(512) copy_probe_kernel(const float4 *__restrict__ src, float4 *__restrict__ dst,
+                                                         int64_t n16) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n16; i += 4 * stride) {
+        const float4 a = __ldcs(src + i), b = __ldcs(src + i + stride), c = __ldcs(src + i + 2 * stride),
+                     d = __ldcs(src + i + 3 * stride);
+        __stcs(dst + i, a);
+        __stcs(dst + i + stride, b);
+        __stcs(dst + i + 2 * stride, c);
+        __stcs(dst + i + 3 * stride, d);
+    }
+    for (; i < n16; i += stride) __stcs(dst + i, __ldcs(src + i));
+}
+
 // ---------------------------------------------------------------- |0...0>
 __global__ void set_amp0_kernel(float2 *state) { state[0] = make_float2(1.0f, 0.0f); }
 __global__ void set_amp0_kernel_d(double2 *state) { state[0] = make_double2(1.0, 0.0); }
@@ -288,6 +306,15 @@ cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm,
         dev::remap_kernel<double2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const double2 *)src, (double2 *)dst, P);
     else
         dev::remap_kernel<float2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const float2 *)src, (float2 *)dst, P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_probe(void *dst, const void *src, size_t bytes, int nsm, cudaStream_t stream) {
+    const int64_t n16 = (int64_t)(bytes / 16);
+    int64_t grid = (int64_t)nsm * 4;
+    if (grid > (n16 + 511) / 512) grid = (n16 + 511) / 512;
+    if (grid < 1) grid = 1;
+    dev::copy_probe_kernel<<<(unsigned)grid, 512, 0, stream>>>((const float4 *)src, (float4 *)dst, n16);
     return cudaGetLastError();
 }
 

@@ -16,6 +16,7 @@ cudaError_t launch_sweep_c128(double2 *state, const QsvSweepD &sw, int nsm, cuda
 cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, int nsm,
                          cudaStream_t stream);
 cudaError_t launch_set_amp0(void *state, int dtype, cudaStream_t stream);
+cudaError_t launch_copy_probe(void *dst, const void *src, size_t bytes, int nsm, cudaStream_t stream);
 cudaError_t launch_reduce(const void *state, int n, int dtype, double *out, void *scratch, cudaStream_t stream);
 cudaError_t launch_chunk_probs(const void *state, int n, int dtype, int cb, double *out, cudaStream_t stream);
 cudaError_t launch_sample(const void *state, int n, int dtype, int cb, const double *uni, int shots, int64_t *out,
@@ -258,6 +259,18 @@ int qsv_sample_f64(const void *state, int n, int dtype, const double *uniforms_d
                                        (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "sample launch");
     t_launches += 3;
+    return QSV_OK;
+}
+
+int qsv_hbm_copy(void *dst, const void *src, size_t bytes, void *stream) {
+    if (!dst || !src) return fail(QSV_ERR_INVALID_ARG, "null pointer");
+    if (bytes % 16 || ((uintptr_t)dst % 16) || ((uintptr_t)src % 16))
+        return fail(QSV_ERR_INVALID_ARG, "copy probe needs 16-byte aligned buffers and a multiple of 16 bytes");
+    const char *d = (const char *)dst, *s = (const char *)src;
+    if (d < s + bytes && s < d + bytes) return fail(QSV_ERR_INVALID_ARG, "copy probe buffers overlap");
+    cudaError_t e = qsv::launch_copy_probe(dst, src, bytes, sm_count(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "copy probe launch");
+    t_launches++;
     return QSV_OK;
 }
 

@@ -71,6 +71,7 @@ def load(path=LIB_PATH):
         "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
         "qsv_jit_wait": ([], I32),
         "qsv_jit_info": ([P, ctypes.c_int], I32),
+        "qsv_hbm_copy": ([P, P, SZ, P], I32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -92,7 +93,7 @@ def exported_symbols():
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
             "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
-            "qsv_jit_wait", "qsv_jit_info"]
+            "qsv_jit_wait", "qsv_jit_info", "qsv_hbm_copy"]
 
 
 def _check(rc):
@@ -323,6 +324,14 @@ def set_layout13(rb):
 
 def set_phase_lanes(k):
     _check(load().qsv_set_phase_lanes(int(k)))
+
+
+def hbm_copy(dst, src, stream=None):
+    """dst <- src with the HBM copy probe kernel (same byte size, 16-byte aligned, distinct tensors)."""
+    nb = src.numel() * src.element_size()
+    if dst.numel() * dst.element_size() != nb:
+        raise ValueError("copy probe tensors differ in size")
+    _check(load().qsv_hbm_copy(_ptr(dst), _ptr(src), nb, _stream(stream)))
 
 
 JIT_MODES = {"off": 0, "eager": 1, "auto": 2}
