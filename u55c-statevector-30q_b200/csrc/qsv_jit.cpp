@@ -221,10 +221,17 @@ bool nvrtc_compile(const std::string &src, std::vector<char> &cubin, std::string
         log = "nvrtcCreateProgram failed";
         return false;
     }
-    // QSV_JIT_PTXAS_VERBOSE=1 keeps ptxas's resource report (registers, spills) in the compile log
-    const bool verbose = std::getenv("QSV_JIT_PTXAS_VERBOSE") != nullptr;
-    const char *opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-DQSV_JIT=1", "--ptxas-options=-v"};
-    const nvrtcResult r = nvrtcCompileProgram(prog, verbose ? 4 : 3, opts);
+    // QSV_JIT_PTXAS_VERBOSE=1 keeps ptxas's resource report (registers, spills) in the compile log;
+    // QSV_JIT_EXTRA_OPTS adds NVRTC options (space separated), for compile-time / code-quality studies
+    std::vector<std::string> extra;
+    if (const char *x = std::getenv("QSV_JIT_EXTRA_OPTS")) {
+        std::istringstream is(x);
+        for (std::string o; is >> o;) extra.push_back(o);
+    }
+    std::vector<const char *> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-DQSV_JIT=1"};
+    if (std::getenv("QSV_JIT_PTXAS_VERBOSE")) opts.push_back("--ptxas-options=-v");
+    for (const std::string &o : extra) opts.push_back(o.c_str());
+    const nvrtcResult r = nvrtcCompileProgram(prog, (int)opts.size(), opts.data());
     size_t ls = 0;
     nvrtcGetProgramLogSize(prog, &ls);
     log.assign(ls, '\0');
