@@ -73,6 +73,20 @@ int groups_for(const QsvSweep &sw, int wb) {
     return dense <= 8 && lane <= 2 ? 2 : 1;
 }
 
+// Whether a sweep's kernel interleaves the phases of two tiles per consumer thread (sweep_pipeline IL).
+// Default: multi-phase tensor-map staged sweeps run by one consumer group (measured on the 30-qubit
+// random-layer program: 2 % faster there; the FP32-bound bulk-staged sweeps over qubits 0-12 ran 5-15 %
+// slower interleaved, so they keep the block-wide barrier). QSV_JIT_INTERLEAVE=0: never; =2: every
+// multi-phase sweep of one consumer group.
+int interleave_for(const QsvSweep &sw, int groups) {
+    static const int mode = [] {
+        const char *e = std::getenv("QSV_JIT_INTERLEAVE");
+        return e ? std::atoi(e) : 1;
+    }();
+    if (mode == 0 || groups != 1 || sw.nphases < 2) return 0;
+    return mode == 2 || sw.tma_rank > 0 ? 1 : 0;
+}
+
 struct Drv {
     PFN_cuModuleLoadData_v2000 module_load = nullptr;
     PFN_cuModuleGetFunction_v2000 get_function = nullptr;
@@ -163,13 +177,15 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
       << "    using Amp = float2;\n"
       << "    static constexpr int kHalfBits = 1;\n"
       << "    static constexpr bool kSmemOps = false;\n"
+      << "    static constexpr int kPhases = " << sw.nphases << ";\n"
+      << "    // one phase of a tile: load in the phase's layout, apply its ops, store\n"
       << "    template <int NV, int RB, int WB>\n"
-      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *, int lane, int warp,\n"
-      << "                                                int bar) {\n";
+      << "    static __device__ __forceinline__ void phase(int p, float2 *tile, const QsvSweep &P, const QsvOp *, int lane,\n"
+      << "                                                 int warp) {\n"
+      << "        switch (p) {\n";
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
-        if (p > 0) s << "        named_bar_sync(bar, " << nc << ");\n";
-        s << "        {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_bits[0] << ", "
+        s << "        case " << p << ": {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_bits[0] << ", "
           << (int)ph.lane_bits[1] << ">(lane)";
         for (int w = 0; w < wb; w++) s << " | jit_warp_bit<" << (int)ph.warp_bits[w] << ">(warp, " << w << ")";
         s << ";\n            float2 R[NV], I[NV];\n";
@@ -203,14 +219,23 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
                 s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb, lane);\n";
         }
-        s << "            jit_store<NV, " << rbits << ">(tile, tb, R, I);\n        }\n";
+        s << "            jit_store<NV, " << rbits << ">(tile, tb, R, I);\n            break;\n        }\n";
     }
-    s << "    }\n};\n}  // namespace dev\n}  // namespace qsv\n"
+    s << "        default: break;\n        }\n    }\n"
+      << "    template <int NV, int RB, int WB>\n"
+      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *ops, int lane, int warp,\n"
+      << "                                                int bar) {\n"
+      << "#pragma unroll\n"
+      << "        for (int p = 0; p < kPhases; p++) {\n"
+      << "            if (p > 0) named_bar_sync(bar, " << nc << ");\n"
+      << "            phase<NV, RB, WB>(p, tile, P, ops, lane, warp);\n"
+      << "        }\n    }\n";
+    s << "};\n}  // namespace dev\n}  // namespace qsv\n"
       << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb << ")\n"
       << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
       << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
       << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages << ", " << groups
-      << ", qsv::dev::JitBody>(state, P, &tmap, status);\n}\n";
+      << ", qsv::dev::JitBody, QsvSweep, " << interleave_for(sw, groups) << ">(state, P, &tmap, status);\n}\n";
     return s.str();
 }
 

@@ -7,7 +7,11 @@
 //     are long; completion is counted on mbarriers, up to S tiles are in flight;
 //   * G groups of consumer warps run Body::tile on the staged tiles (the ops of the sweep, in registers);
 //     with G = 2 the groups take alternate tiles, so one group's phase barriers and shared-memory round
-//     trips overlap the other group's arithmetic.
+//     trips overlap the other group's arithmetic;
+//   * or (IL = 1, one group) every consumer thread keeps two tiles in flight and interleaves their phases
+//     (Body::phase), with an mbarrier per tile slot in place of the block-wide barrier between two phases of
+//     a tile: a thread runs a phase of the other tile while the slowest threads finish their stores, so the
+//     phase round trips of one tile overlap the arithmetic of the other without a second register set.
 // Body is the interpreter (qsv_sweep.cu: op table read at run time) or a kernel specialised to one sweep
 // structure (qsv_jit.cpp: ops fixed at compile time). Both run the same arithmetic (qsv_ops.cuh).
 // The tile addressing is the reference's (host/sv/model.py:25-40, sv_engine.cpp:61-84,116): tile T's
@@ -74,8 +78,9 @@ __host__ __device__ constexpr size_t sweep_smem_bytes() {
 // The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S, Body, SW>() bytes
 // of dynamic shared memory. status: device word that bounded waits OR their failure bit into.
 // Body::Amp is the amplitude type (float2: complex64, double2: complex128); Body::kHalfBits is 1 when a
-// thread's 16-byte slot packs two amplitudes (tile bit 0), 0 when it holds one.
-template <int KW, int RB, int WB, int S, int G, class Body, class SW = QsvSweep>
+// thread's 16-byte slot packs two amplitudes (tile bit 0), 0 when it holds one. IL = 1 needs G = 1 and a
+// Body with kPhases and phase(p, ...) (one phase of a tile: load in its layout, apply its ops, store).
+template <int KW, int RB, int WB, int S, int G, class Body, class SW = QsvSweep, int IL = 0>
 __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ state, const SW &P,
                                                const CUtensorMap *tmap, int *status) {
     using Amp = typename Body::Amp;
@@ -97,6 +102,7 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
     constexpr int NF = S * G;
     __shared__ __align__(8) uint64_t full[NF];
     __shared__ __align__(8) uint64_t done[S];
+    __shared__ __align__(8) uint64_t pbar[2];     // IL: phase barriers of the two tiles in flight
     __shared__ volatile int abort_flag;
 
     const int tid = threadIdx.x;
@@ -109,6 +115,7 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
     if (tid == 0) {
         for (int f = 0; f < NF; f++) mbar_init(&full[f], 1);
         for (int s = 0; s < S; s++) mbar_init(&done[s], NCG);
+        for (int u = 0; u < 2; u++) mbar_init(&pbar[u], NCG);
         abort_flag = 0;
         fence_mbar_init();
     }
@@ -199,6 +206,42 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
     }
 
     // ---------------------------------------------------------------- consumer warps
+    if constexpr (IL != 0) {
+        static_assert(G == 1, "interleaved phases run one consumer group");
+        // tiles j0 and j0 + 1 (slots u = 0, 1): phase p of both, then phase p + 1 of both. Every consumer
+        // thread arrives on pbar[u] after its stores of a phase and waits on it before its loads of the next
+        // phase of the same tile; it waits on each completion of pbar[u] in order, so its count of waits gives
+        // the parity, and no thread can fall two completions behind (each completion needs its arrival).
+        const int lane = tid & 31, warp = tid >> 5;
+        uint32_t waits[2] = {0u, 0u};
+        bool ok = true;
+        for (int64_t j0 = 0; ok && j0 < nmine; j0 += 2) {
+            const int cnt = j0 + 1 < nmine ? 2 : 1;
+#pragma unroll
+            for (int p = 0; p < Body::kPhases; p++) {
+                for (int u = 0; u < cnt; u++) {
+                    const int64_t j = j0 + u;
+                    const int b = (int)(j % S);
+                    if (p == 0) {
+                        ok = mbar_wait(&full[j % NF], (uint32_t)((j / NF) & 1), &abort_flag, status);
+                    } else {
+                        ok = mbar_wait(&pbar[u], waits[u] & 1u, &abort_flag, status);
+                        waits[u]++;
+                    }
+                    if (!ok) break;
+                    Body::template phase<NV, RB, WB>(p, bufs + (size_t)b * TILE, P, sops, lane, warp);
+                    if (p + 1 < Body::kPhases) {
+                        mbar_arrive(&pbar[u]);
+                    } else {
+                        fence_proxy_async_smem();
+                        mbar_arrive(&done[b]);
+                    }
+                }
+                if (!ok) break;
+            }
+        }
+        return;
+    }
     const int grp = tid / NCG;                   // group grp takes tiles grp, grp + G, ...
     const int lane = tid & 31, warp = (tid % NCG) >> 5;
     for (int64_t j = grp; j < nmine; j += G) {
