@@ -61,21 +61,28 @@ def _plan_ops_phys(plan):
             for o in range(ph["op_begin"], ph["op_end"]):
                 op = sw["ops"][o]
                 tb = op["tbit"]
+                # lane bits 0-2: tile bits 1-3, or in a swizzled sweep one of each pair (1+l, 4+l)
+                if sw["swizzled"]:
+                    assert all(ph["lane_lo"][l] in (1 + l, 4 + l) for l in range(3)), ph["lane_lo"]
+                else:
+                    assert ph["lane_lo"] == [1, 2, 3]
                 # slot placement
                 if tb == 0:
                     assert op["slot"] == 0
-                elif tb < 4:
-                    assert op["slot"] == 8 + tb - 1
+                elif tb in ph["lane_lo"]:
+                    assert op["slot"] == 8 + ph["lane_lo"].index(tb)
                 elif tb in ph["reg_bits"]:
                     assert op["slot"] == 1 + ph["reg_bits"].index(tb)
                 else:
                     assert tb in ph["lane_bits"] and op["slot"] == 11 + ph["lane_bits"].index(tb)
                 # the phase layout covers every tile bit exactly once
-                bits = sorted([0, 1, 2, 3] + ph["reg_bits"] + ph["lane_bits"] + ph["warp_bits"])
+                bits = sorted([0] + ph["lane_lo"] + ph["reg_bits"] + ph["lane_bits"] + ph["warp_bits"])
                 assert bits == list(range(sw["kw"])), bits
                 assert len(ph["reg_bits"]) == rb
                 ctrls = frozenset(W[b] for b in range(sw["kw"]) if (op["cmask"] >> b) & 1)
                 out.append((W[tb], ctrls, tuple(op["m0"].view(np.int32)), tuple(op["m1"].view(np.int32))))
+        if sw["swizzled"]:                       # staged by 128-byte-swizzled tensor-map boxes
+            assert sw["tma_rank"] > 0 and sw["tdim_box"][0] == 4 and sw["lo"] >= 4
         assert sw["lo"] >= 3 and len(W) == sw["kw"] and len(set(W)) == sw["kw"]
         assert W == sorted(W)
     return out

@@ -146,3 +146,58 @@ def test_auto_mode_switches_without_changing_values(torch, jit_mode):
     info = engine.jit_info()
     assert engine.device_status() == 0
     assert info["failed"] == 0 and info["jit_launches"] > before
+
+
+_SWITCH_SCRIPT = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import conftest  # noqa: F401  (registers the package as qsv_b200)
+import numpy as np, torch
+import qsv_b200 as q
+from qsv_b200 import engine, generators as gen
+from oracle import oracle as orc
+engine.load()
+swizzled = 0
+for n, maker in ((14, lambda: gen.random_layer(14, 8, 13)), (20, lambda: gen.random_layer(20, 10, 0)),
+                 (24, lambda: gen.random_layer_ccx(24, 4, 15))):
+    prog, _, _ = q.compile_circuit(maker(), n, 12)
+    segs = [s for kind, s in prog if kind == "segment"]
+    swizzled += sum(sw["swizzled"] for s in segs for sw in engine.plan_segment(s, n))
+    rng = np.random.default_rng(n)
+    x = (rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)).astype(np.complex64)
+    outs = []
+    for mode in ("off", "eager"):
+        engine.set_jit(mode)
+        t = torch.from_numpy(x.copy()).cuda()
+        for s in segs:
+            engine.run_segment(t, s)
+        torch.cuda.synchronize()
+        outs.append(t.cpu().numpy())
+    assert engine.device_status() == 0
+    assert np.array_equal(outs[0], outs[1]), n
+    if n <= 20:
+        ref = x.copy()
+        for s in segs:
+            ref = orc.run_segment(ref, s)
+        assert np.array_equal(outs[1], ref), n
+print("swizzled sweeps", swizzled)
+"""
+
+
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("env", [{"QSV_JIT_INTERLEAVE": "2"}, {"QSV_SWIZZLE": "0", "QSV_JIT_INTERLEAVE": "1"}])
+def test_layout_switches_exact(torch, env, tmp_path):
+    """The non-default layout switches (read once per process, so run in a child process): phases of two
+    tiles interleaved in every multi-phase sweep; no swizzled layouts with interleaved tensor-map sweeps.
+    Specialised == interpreter == oracle, exactly."""
+    import os
+    import subprocess
+    import sys
+    tests_dir = os.path.dirname(os.path.abspath(__file__))
+    script = tmp_path / "switches.py"
+    script.write_text(_SWITCH_SCRIPT)
+    r = subprocess.run([sys.executable, str(script), tests_dir], env={**os.environ, **env},
+                       capture_output=True, text=True, timeout=800)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    swz = int(r.stdout.split("swizzled sweeps")[1])
+    assert (swz == 0) == (env.get("QSV_SWIZZLE") == "0"), r.stdout

@@ -74,14 +74,14 @@ int groups_for(const QsvSweep &sw, int wb) {
 }
 
 // Whether a sweep's kernel interleaves the phases of two tiles per consumer thread (sweep_pipeline IL).
-// Default: multi-phase tensor-map staged sweeps run by one consumer group (measured on the 30-qubit
-// random-layer program: 2 % faster there; the FP32-bound bulk-staged sweeps over qubits 0-12 ran 5-15 %
-// slower interleaved, so they keep the block-wide barrier). QSV_JIT_INTERLEAVE=0: never; =2: every
+// Off by default: on the 30-qubit random-layer program it made the tensor-map sweeps with 7-8 dense ops
+// 0.5-2 % faster and the FP32-bound sweeps over qubits 0-12 5-15 % slower (their prefetch depth drops from
+// two tiles to one). QSV_JIT_INTERLEAVE=1: multi-phase tensor-map sweeps of one consumer group; =2: every
 // multi-phase sweep of one consumer group.
 int interleave_for(const QsvSweep &sw, int groups) {
     static const int mode = [] {
         const char *e = std::getenv("QSV_JIT_INTERLEAVE");
-        return e ? std::atoi(e) : 1;
+        return e ? std::atoi(e) : 0;
     }();
     if (mode == 0 || groups != 1 || sw.nphases < 2) return 0;
     return mode == 2 || sw.tma_rank > 0 ? 1 : 0;
@@ -151,10 +151,11 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
     std::string k;
     auto put = [&](int v) { k.push_back((char)(v & 0xff)); };
     auto put32 = [&](uint32_t v) { k.append(reinterpret_cast<const char *>(&v), 4); };
-    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops);
+    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops); put(sw.swz);
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
         for (int r = 0; r < rb; r++) put(ph.reg_bits[r]);
+        for (int l = 0; l < 3; l++) put(ph.lane_lo[l]);
         put(ph.lane_bits[0]); put(ph.lane_bits[1]);
         for (int w = 0; w < wb; w++) put(ph.warp_bits[w]);
         put(ph.op_begin); put(ph.op_end);
@@ -185,13 +186,14 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
       << "        switch (p) {\n";
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
-        s << "        case " << p << ": {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_bits[0] << ", "
+        s << "        case " << p << ": {\n            const uint32_t tb = jit_lane_base<" << (int)ph.lane_lo[0] << ", "
+          << (int)ph.lane_lo[1] << ", " << (int)ph.lane_lo[2] << ", " << (int)ph.lane_bits[0] << ", "
           << (int)ph.lane_bits[1] << ">(lane)";
         for (int w = 0; w < wb; w++) s << " | jit_warp_bit<" << (int)ph.warp_bits[w] << ">(warp, " << w << ")";
         s << ";\n            float2 R[NV], I[NV];\n";
         std::string rbits;
         for (int r = 0; r < rb; r++) rbits += (r ? ", " : "") + std::to_string((int)ph.reg_bits[r]);
-        s << "            jit_load<NV, " << rbits << ">(tile, tb, R, I);\n";
+        s << "            jit_load<NV, " << (int)sw.swz << ", " << rbits << ">(tile, tb, R, I);\n";
         for (int o = ph.op_begin; o < ph.op_end; o++) {
             const QsvOp &op = sw.ops[o];
             const std::string thr = std::to_string(op.cm_thr) + "u";
@@ -219,7 +221,7 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
                 s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb, lane);\n";
         }
-        s << "            jit_store<NV, " << rbits << ">(tile, tb, R, I);\n            break;\n        }\n";
+        s << "            jit_store<NV, " << (int)sw.swz << ", " << rbits << ">(tile, tb, R, I);\n            break;\n        }\n";
     }
     s << "        default: break;\n        }\n    }\n"
       << "    template <int NV, int RB, int WB>\n"
@@ -458,7 +460,8 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
     const int NT = e->groups * (1 << (5 + wb)) + 32;
-    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2);
+    // sweep_smem_bytes of the generated body: the tile buffers plus 1 KiB for their 1024-byte alignment
+    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN;
     if (!e->fn[dev]) {
         // loading a module is not a stream operation: keep it out of stream captures
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;

@@ -14,10 +14,11 @@
 namespace qsv {
 namespace dev {
 
-// thread base of a phase: tile bits 1-3 from lane bits 0-2, lane bits 3-4 on tile bits LB0 / LB1
-template <int LB0, int LB1>
+// thread base of a phase: lane bits 0-2 on tile bits L0-L2, lane bits 3-4 on tile bits LB0 / LB1
+template <int L0, int L1, int L2, int LB0, int LB1>
 __device__ __forceinline__ uint32_t jit_lane_base(int lane) {
-    return ((uint32_t)(lane & 7) << 1) | ((uint32_t)((lane >> 3) & 1) << LB0) | ((uint32_t)((lane >> 4) & 1) << LB1);
+    return ((uint32_t)(lane & 1) << L0) | ((uint32_t)((lane >> 1) & 1) << L1) | ((uint32_t)((lane >> 2) & 1) << L2) |
+           ((uint32_t)((lane >> 3) & 1) << LB0) | ((uint32_t)((lane >> 4) & 1) << LB1);
 }
 template <int WBIT>
 __device__ __forceinline__ uint32_t jit_warp_bit(int warp, int w) {
@@ -34,20 +35,28 @@ __device__ __forceinline__ constexpr uint32_t jit_reg_off(int r) {
     return o;
 }
 
-template <int NV, int... RBITS>
+// SWZ: the tile is stored with the 128-byte swizzle (swz128); the thread base and the register offsets
+// (disjoint bits) are swizzled separately and combined with XOR, the offsets at compile time
+template <int NV, int SWZ, int... RBITS>
 __device__ __forceinline__ void jit_load(const float2 *tile, uint32_t tb, float2 (&R)[NV], float2 (&I)[NV]) {
+    const uint32_t base = SWZ ? swz128(tb) : tb;
 #pragma unroll
     for (int r = 0; r < NV; r++) {
-        const float4 v = *reinterpret_cast<const float4 *>(tile + tb + jit_reg_off<RBITS...>(r));
+        const uint32_t off = jit_reg_off<RBITS...>(r);
+        const float4 v = *reinterpret_cast<const float4 *>(tile + (base ^ (SWZ ? swz128(off) : off)));
         R[r] = make_float2(v.x, v.z);
         I[r] = make_float2(v.y, v.w);
     }
 }
-template <int NV, int... RBITS>
+template <int NV, int SWZ, int... RBITS>
 __device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float2 (&R)[NV], const float2 (&I)[NV]) {
+    const uint32_t base = SWZ ? swz128(tb) : tb;
 #pragma unroll
-    for (int r = 0; r < NV; r++)
-        *reinterpret_cast<float4 *>(tile + tb + jit_reg_off<RBITS...>(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+    for (int r = 0; r < NV; r++) {
+        const uint32_t off = jit_reg_off<RBITS...>(r);
+        *reinterpret_cast<float4 *>(tile + (base ^ (SWZ ? swz128(off) : off))) =
+            make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+    }
 }
 
 __device__ __forceinline__ void jit_mat(float (&m)[8], const float *src) {

@@ -442,12 +442,19 @@ __device__ __forceinline__ void apply_op(const QsvOp &op, float2 (&R)[NV], float
     }
 }
 
+// Shared-memory position of tile index x in a swizzled tile (the tensor map's 128-byte swizzle: the 16-byte
+// chunk index, tile bits 1-3, is XORed with tile bits 4-6). Linear over XOR, so a thread's base and a
+// register offset (disjoint bits) can be swizzled separately.
+__device__ __forceinline__ uint32_t swz128(uint32_t x) { return x ^ ((x >> 3) & 0xEu); }
+
 // One phase of a tile in shared memory: read the thread's 2^RB float4 in the phase's layout, apply ops
-// [op_begin, op_end), write them back. PH is any phase record with reg_bits / lane_bits / warp_bits.
+// [op_begin, op_end), write them back. PH is any phase record with reg_bits / lane_lo / lane_bits /
+// warp_bits; swz: the tile is stored swizzled.
 template <int NV, int RB, int WB, class PH>
 __device__ __forceinline__ void run_phase(float2 *tile, const PH &Q, const QsvOp *ops, int op_begin, int op_end,
-                                          int lane, int warp) {
-    uint32_t tb = ((uint32_t)(lane & 7) << 1) | ((uint32_t)((lane >> 3) & 1) << Q.lane_bits[0]) |
+                                          int lane, int warp, bool swz = false) {
+    uint32_t tb = ((uint32_t)(lane & 1) << Q.lane_lo[0]) | ((uint32_t)((lane >> 1) & 1) << Q.lane_lo[1]) |
+                  ((uint32_t)((lane >> 2) & 1) << Q.lane_lo[2]) | ((uint32_t)((lane >> 3) & 1) << Q.lane_bits[0]) |
                   ((uint32_t)((lane >> 4) & 1) << Q.lane_bits[1]);
 #pragma unroll
     for (int w = 0; w < WB; w++) tb |= (uint32_t)((warp >> w) & 1) << Q.warp_bits[w];
@@ -461,17 +468,18 @@ __device__ __forceinline__ void run_phase(float2 *tile, const PH &Q, const QsvOp
             if ((r >> q) & 1) o |= rbit[q];
         return o;
     };
+    auto addr = [&](int r) -> uint32_t { return swz ? swz128(pos(r)) : pos(r); };
     float2 R[NV], I[NV];
 #pragma unroll
     for (int r = 0; r < NV; r++) {
-        const float4 v = *reinterpret_cast<const float4 *>(tile + pos(r));
+        const float4 v = *reinterpret_cast<const float4 *>(tile + addr(r));
         R[r] = make_float2(v.x, v.z);
         I[r] = make_float2(v.y, v.w);
     }
     for (int o = op_begin; o < op_end; o++) apply_op<NV, RB>(ops[o], R, I, tb, lane);
 #pragma unroll
     for (int r = 0; r < NV; r++)
-        *reinterpret_cast<float4 *>(tile + pos(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+        *reinterpret_cast<float4 *>(tile + addr(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
 }
 
 }  // namespace dev

@@ -44,6 +44,7 @@ typedef unsigned long long uint64_t;
 #define QSV_MAX_PHASES 24
 #define QSV_LO_MIN 3            // smallest sub-block: 2^3 amplitudes = 64 bytes (QSV2 guarantees k-m >= 3)
 #define QSV_TMA_TENSOR_LO 9     // sub-blocks shorter than 2^9 amplitudes are staged with a tensor-map box
+#define QSV_SMEM_ALIGN 1024     // sweep kernels align their tile buffers to this in dynamic shared memory
 #define QSV_TMA_MAX_RANK 5
 
 // matrix classes (host-detected, exact comparisons). The specialised forms give the same values as the
@@ -119,12 +120,15 @@ struct QsvOpD {
     uint8_t pad[6];
 };
 
+// A phase's thread layout: lane bits 0-2 sit on tile bits lane_lo[0..2] (1, 2, 3 for complex64 unless the
+// sweep is swizzled, see QsvSweepT::swz; 0, 1, 2 for complex128), lane bits 3-4 on lane_bits[0..1].
 struct QsvPhase {
     uint8_t reg_bits[QSV_RB_MAX];
     uint8_t lane_bits[2];
     uint8_t warp_bits[QSV_WB_MAX];
     uint8_t op_begin, op_end;
-    uint8_t pad[4];
+    uint8_t lane_lo[3];
+    uint8_t pad[1];
 };
 
 // phase with 32-bit op indices (whole-circuit programs of the batch kernel can exceed 255 ops)
@@ -132,7 +136,8 @@ struct QsvPhaseX {
     uint8_t reg_bits[QSV_RB_MAX];
     uint8_t lane_bits[2];
     uint8_t warp_bits[QSV_WB_MAX];
-    uint8_t pad[2];
+    uint8_t lane_lo[3];
+    uint8_t pad[3];
     int32_t op_begin, op_end;
 };
 
@@ -147,7 +152,11 @@ struct QsvSweepT {
     uint8_t tma_rank;           // 0: bulk copies per sub-block; 2..5: one tensor-map box per tile
     uint8_t tdim_free[QSV_TMA_MAX_RANK];   // free bits of T folded into each tensor dim (low dim first)
     uint8_t tdim_box[QSV_TMA_MAX_RANK];    // log2 box extent of each tensor dim
-    uint8_t pad[4];
+    // 1: the tile sits in shared memory with the 128-byte swizzle of the tensor-map copies (16-byte chunk
+    // index = tile bits 1-3 XOR tile bits 4-6), so lane bit l may sit on tile bit 1+l or 4+l without bank
+    // conflicts and ops on tile bits 1-3 can run in registers (complex64 tensor-map sweeps only)
+    uint8_t swz;
+    uint8_t pad[3];
     int64_t ntiles;             // 2^(n - kw)
     int32_t nphases;
     int32_t nops;

@@ -7,6 +7,7 @@
 #include "qsv_planner.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -102,6 +103,15 @@ int set_phase_lanes(int k) {
     return 0;
 }
 
+// swizzled layouts for complex64 tensor-map sweeps (QsvSweepT::swz): on unless QSV_SWIZZLE=0
+static bool swizzle_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("QSV_SWIZZLE");
+        return !(e && std::atoi(e) == 0);
+    }();
+    return on;
+}
+
 int set_rb13(int rb) {
     if (rb != 3 && rb != 4) return -1;
     g_rb13 = rb;
@@ -160,16 +170,19 @@ static void set_mats(QsvOpD &o, const PhysOp &p) {
 
 // Tensor-map staging for windows with short contiguous runs: one dim per chunk (<= 8 bits) of each run of
 // window bits, each spanning the free bits up to the next window bit. Returns the rank, 0 if it does not fit.
+// swz: the map of a swizzled sweep, whose first dim is exactly tile bits 0-3 (128-byte rows, the span of
+// the 128-byte swizzle); needs lo >= 4, any lo.
 template <class SW>
-static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart) {
-    if (sw.lo >= QSV_TMA_TENSOR_LO) return 0;
+static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart, bool swz = false) {
+    if (swz ? sw.lo < 4 : sw.lo >= QSV_TMA_TENSOR_LO) return 0;
     int wb[QSV_KW_MAX], nw = 0;            // window bits ascending
     for (int q = 0; q < sw.lo; q++) wb[nw++] = q;
     for (int i = 0; i < sw.nh; i++) wb[nw++] = sw.H[i];
     int rank = 0, i = 0;
     while (i < nw) {
+        const int maxlen = (swz && rank == 0) ? 4 : 8;
         int start = wb[i], len = 1;
-        while (i + len < nw && wb[i + len] == start + len && len < 8) len++;
+        while (i + len < nw && wb[i + len] == start + len && len < maxlen) len++;
         const int next = (i + len < nw) ? wb[i + len] : sw.n;
         const int fr = next - (start + len);
         if (rank == QSV_TMA_MAX_RANK || len + fr > 31) return 0;
@@ -186,9 +199,13 @@ static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart
 // Phases are greedy in op order: tile bits above the fixed lane bits (>= 4 for complex64, whose tile bit 0
 // is the packed half of a float4 and bits 1-3 are lanes; >= 3 for complex128, bits 0-2 lanes) that are
 // targets need a register or lane slot.
+// swz (complex64 only): the swizzled layout, in which lane bit l (0-2) sits on tile bit 1+l or 4+l, chosen
+// per phase, so tile bits 1-3 need slots like the others and can be register bits; lane_cap bounds its
+// lane-bit targets (warp-shuffle ops) per phase.
 template <class OpT>
 static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n, int kw,
-                       std::vector<OpT> &out, std::vector<QsvPhaseX> &phases, std::string &err) {
+                       std::vector<OpT> &out, std::vector<QsvPhaseX> &phases, std::string &err, bool swz = false,
+                       int lane_cap = 8) {
     constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
     constexpr int FIXED_LO = C128 ? 0 : 1;       // first tile bit on lane bits 0-2
     constexpr int FREE_LO = FIXED_LO + 3;        // tile bits from here on need a slot when targeted
@@ -235,44 +252,90 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             o.variant = QSV_V_MUX;
         }
     }
-    const int cap = rb + g_phase_lanes;
+    if (C128) swz = false;
     const size_t nops = out.size();
+    // swizzled layout: tile bits 1+l and 4+l pair up on lane bit l
+    auto pair_of = [&](int t) { return (swz && t >= 1 && t <= 6) ? (t - 1) % 3 : -1; };
+    auto partner_of = [](int t) { return t <= 3 ? t + 3 : t - 3; };
+    struct Assign {
+        int regs[QSV_RB_MAX], nr;   // register-bit targets, most used first
+        int pl[3];                  // swizzled: target on lane bit l (a pair member), -1 if none
+        int fl[2], nf;              // targets on lane bits 3-4
+    };
+    // slots for a phase's targets, most used first: a register bit (unless the target's pair partner holds
+    // one: lane bit l must stay on one of the pair), else the pair's lane bit, else a free lane bit (at most
+    // g_phase_lanes of them). False if they do not fit. Without swz this is the plain capacity rule
+    // rb + g_phase_lanes over tile bits >= FREE_LO, whose lane bits 0-2 are fixed.
+    auto assign = [&](const int *used, const int *cnt, int nu, Assign &A) -> bool {
+        int order[QSV_KW_MAX];
+        for (int u = 0; u < nu; u++) order[u] = u;
+        std::stable_sort(order, order + nu, [&](int x, int y) { return cnt[x] > cnt[y]; });
+        A.nr = 0;
+        A.nf = 0;
+        A.pl[0] = A.pl[1] = A.pl[2] = -1;
+        for (int k = 0; k < nu; k++) {
+            const int t = used[order[k]];
+            const int l = pair_of(t);
+            bool partner_reg = false;
+            if (l >= 0)
+                for (int r = 0; r < A.nr; r++) partner_reg |= A.regs[r] == partner_of(t);
+            const int nlane = A.nf + (A.pl[0] >= 0) + (A.pl[1] >= 0) + (A.pl[2] >= 0);
+            if (A.nr < rb && !partner_reg) A.regs[A.nr++] = t;
+            else if (l >= 0 && A.pl[l] < 0 && nlane < lane_cap) A.pl[l] = t;
+            else if (A.nf < g_phase_lanes && nlane < lane_cap) A.fl[A.nf++] = t;
+            else return false;
+        }
+        return true;
+    };
+    const int need_lo = swz ? 1 : FREE_LO;      // targets from this tile bit on need a slot
     size_t i = 0;
     while (i < nops) {
         size_t j = i;
         int used[QSV_KW_MAX], cnt[QSV_KW_MAX], nu = 0;
+        Assign A, B;
+        assign(used, cnt, 0, A);
         while (j < nops) {
             const int tb = out[j].tbit;
-            if (tb >= FREE_LO) {
+            if (tb >= need_lo) {
                 int f = -1;
                 for (int u = 0; u < nu; u++)
                     if (used[u] == tb) f = u;
                 if (f < 0) {
-                    if (nu == cap) break;
-                    used[nu] = tb; cnt[nu] = 0; f = nu++;
+                    used[nu] = tb;
+                    cnt[nu] = 0;
+                    if (!assign(used, cnt, nu + 1, B)) break;
+                    A = B;
+                    f = nu++;
                 }
                 cnt[f]++;
             }
             j++;
         }
-        // order targets by use count (stable): most used go to register bits
-        int order[QSV_KW_MAX];
-        for (int u = 0; u < nu; u++) order[u] = u;
-        std::stable_sort(order, order + nu, [&](int x, int y) { return cnt[x] > cnt[y]; });
+        // final slots with the phase's use counts (the fit does not depend on the order; keep the last
+        // fitting assignment should it differ)
+        if (assign(used, cnt, nu, B)) A = B;
         QsvPhaseX ph;
         std::memset(&ph, 0, sizeof(ph));
         bool taken[QSV_KW_MAX] = {false};
-        int slots[QSV_KW_MAX], ns = 0;
-        for (int u = 0; u < nu; u++) { slots[ns++] = used[order[u]]; taken[used[order[u]]] = true; }
-        // targets beyond rb go to lane slots; unused reg/lane slots and warp slots get the remaining bits
-        int regs[QSV_RB_MAX], nr = 0, lanes[2], nl = 0;
-        for (int u = 0; u < ns; u++) {
-            if (nr < rb) regs[nr++] = slots[u];
-            else lanes[nl++] = slots[u];
+        for (int r = 0; r < A.nr; r++) taken[A.regs[r]] = true;
+        for (int f = 0; f < A.nf; f++) taken[A.fl[f]] = true;
+        for (int l = 0; l < 3; l++) {
+            int t = FIXED_LO + l;
+            if (swz) {
+                if (A.pl[l] >= 0) t = A.pl[l];
+                else t = taken[1 + l] ? 4 + l : 1 + l;
+            }
+            ph.lane_lo[l] = (uint8_t)t;
+            taken[t] = true;
         }
+        // unused register / lane slots and the warp slots take the remaining bits
+        int regs[QSV_RB_MAX], nr = 0, lanes[2], nl = 0;
+        for (int r = 0; r < A.nr; r++) regs[nr++] = A.regs[r];
+        for (int f = 0; f < A.nf; f++) lanes[nl++] = A.fl[f];
         int rest[QSV_KW_MAX], nrest = 0;
-        for (int t = FREE_LO; t < kw; t++)
+        for (int t = need_lo; t < kw; t++)
             if (!taken[t]) rest[nrest++] = t;
+        if (nrest != (rb - nr) + (2 - nl) + wb) { err = "internal: layout does not cover the window"; return QSV_ERR_UNSUPPORTED; }
         int ri = 0;
         while (nr < rb) regs[nr++] = rest[ri++];
         while (nl < 2) lanes[nl++] = rest[ri++];
@@ -284,15 +347,19 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
         ph.op_end = (int32_t)j;
         uint32_t regmask = 0;
         for (int r = 0; r < rb; r++) regmask |= 1u << ph.reg_bits[r];
+        uint32_t lanemask = (1u << ph.lane_bits[0]) | (1u << ph.lane_bits[1]);
+        for (int l = 0; l < 3; l++) lanemask |= 1u << ph.lane_lo[l];
         for (size_t o = i; o < j; o++) {
             OpT &op = out[o];
             const int tb = op.tbit;
-            if (!C128 && tb == 0) op.slot = QSV_SLOT_COMP;
-            else if (tb < FREE_LO) op.slot = (uint8_t)(QSV_SLOT_LANE0 + tb - FIXED_LO);
-            else {
+            if (!C128 && tb == 0) {
+                op.slot = QSV_SLOT_COMP;
+            } else {
                 op.slot = 0xff;
                 for (int r = 0; r < rb; r++)
                     if (ph.reg_bits[r] == tb) op.slot = (uint8_t)(QSV_SLOT_REG0 + r);
+                for (int l = 0; l < 3; l++)
+                    if (ph.lane_lo[l] == tb) op.slot = (uint8_t)(QSV_SLOT_LANE0 + l);
                 for (int l = 0; l < 2; l++)
                     if (ph.lane_bits[l] == tb) op.slot = (uint8_t)(QSV_SLOT_LANE0 + 3 + l);
                 if (op.slot == 0xff) { err = "internal: target not placed"; return QSV_ERR_UNSUPPORTED; }
@@ -304,7 +371,6 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             op.cm_thr = op.cmask & ~regmask & (C128 ? ~0u : ~1u);
             // controls on lane bits make the selection differ between the lanes of a warp: take the
             // branch-free form of the controlled variants there
-            const uint32_t lanemask = (C128 ? 0x7u : 0xEu) | (1u << ph.lane_bits[0]) | (1u << ph.lane_bits[1]);
             if (op.cm_thr & lanemask) {
                 if (op.variant == QSV_V_CTRL_DENSE) op.variant = QSV_V_CTRL_DENSE_SEL;
                 else if (op.variant == QSV_V_CTRL_DIAG1) op.variant = QSV_V_CTRL_DIAG1_SEL;
@@ -350,6 +416,31 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
     std::vector<QsvPhaseX> vph;
     int rc = plan_window<OpT>(ops, b, e, tile_of, n, kw, vops, vph, err);
     if (rc) return rc;
+    // the swizzled layout where it costs less: cost = lane ops + 2 per phase change (a shared-memory round
+    // trip moves as many bytes through the shared-memory pipe as two shuffle ops); ties keep the plain one
+    if (!C128 && swizzle_enabled()) {
+        uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
+        const int r = tma_dims(sw, tfree, tbox, tstart, true);
+        auto cost = [](const std::vector<OpT> &o, const std::vector<QsvPhaseX> &p) {
+            int lane = 0;
+            for (const OpT &x : o) lane += x.slot >= QSV_SLOT_LANE0 && x.variant != QSV_V_SKIP;
+            return lane + 2 * ((int)p.size() - 1);
+        };
+        // phases with fewer shuffle ops but more round trips, or the reverse: try lane-op budgets per phase
+        for (int cap : {0, 1, 2, 8}) {
+            std::vector<OpT> sops;
+            std::vector<QsvPhaseX> sph;
+            std::string serr;
+            if (r && plan_window<OpT>(ops, b, e, tile_of, n, kw, sops, sph, serr, true, cap) == QSV_OK &&
+                sph.size() <= QSV_MAX_PHASES && cost(sops, sph) < cost(vops, vph)) {
+                vops.swap(sops);
+                vph.swap(sph);
+                sw.swz = 1;
+                sw.tma_rank = (uint8_t)r;
+                for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
+            }
+        }
+    }
     if (vops.size() > QSV_MAX_SWEEP_OPS || vph.size() > QSV_MAX_PHASES) { err = "sweep too large"; return QSV_ERR_UNSUPPORTED; }
     sw.nops = (int)vops.size();
     sw.nphases = (int)vph.size();
@@ -360,6 +451,7 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         std::memcpy(d.reg_bits, x.reg_bits, sizeof(d.reg_bits));
         std::memcpy(d.lane_bits, x.lane_bits, sizeof(d.lane_bits));
         std::memcpy(d.warp_bits, x.warp_bits, sizeof(d.warp_bits));
+        std::memcpy(d.lane_lo, x.lane_lo, sizeof(d.lane_lo));
         d.op_begin = (uint8_t)x.op_begin;
         d.op_end = (uint8_t)x.op_end;
     }
@@ -424,6 +516,7 @@ int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
         w.push_back(s.tma_rank);
         for (int d = 0; d < QSV_TMA_MAX_RANK; d++) w.push_back(d < s.tma_rank ? s.tdim_free[d] : -1);
         for (int d = 0; d < QSV_TMA_MAX_RANK; d++) w.push_back(d < s.tma_rank ? s.tdim_box[d] : -1);
+        w.push_back(s.swz);
         w.push_back(s.nphases); w.push_back(s.nops);
         for (int p = 0; p < s.nphases; p++) {
             const QsvPhase &ph = s.phases[p];
@@ -431,6 +524,7 @@ int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
             w.push_back(ph.lane_bits[0]); w.push_back(ph.lane_bits[1]);
             for (int r = 0; r < QSV_WB_MAX; r++) w.push_back(r < wb ? ph.warp_bits[r] : -1);
             w.push_back(ph.op_begin); w.push_back(ph.op_end);
+            for (int l = 0; l < 3; l++) w.push_back(ph.lane_lo[l]);
         }
         for (int o = 0; o < s.nops; o++) {
             const QsvOp &op = s.ops[o];

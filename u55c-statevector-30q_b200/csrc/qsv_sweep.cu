@@ -39,7 +39,7 @@ struct InterpBody {
         for (int ph = 0; ph < P.nphases; ph++) {
             if (ph > 0) named_bar_sync(bar, NC);
             const QsvPhase &Q = P.phases[ph];
-            run_phase<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp);
+            run_phase<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp, P.swz != 0);
         }
     }
 };
@@ -80,9 +80,11 @@ cudaError_t make_tmap(CUtensorMap *map, float2 *state, const QsvSweep &sw) {
         estr[d] = 1;
         start += sw.tdim_box[d] + sw.tdim_free[d];
     }
+    // a swizzled sweep's first dim is tile bits 0-3: 16 amplitudes = 128-byte rows, the 128-byte swizzle's span
+    if (sw.swz && (sw.tdim_box[0] != 4 || sw.tma_rank < 2)) return cudaErrorInvalidValue;
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_INT64, sw.tma_rank, state, dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, sw.swz ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 

@@ -68,11 +68,13 @@ __device__ __forceinline__ void tma_store(const CUtensorMap *map, const int32_t 
     }
 }
 
-// Dynamic shared memory a sweep kernel needs: S tile buffers, plus the op table when Body reads it there.
+// Dynamic shared memory a sweep kernel needs: S tile buffers, plus the op table when Body reads it there,
+// plus 1 KiB to align the buffers to 1024 bytes (the 128-byte swizzle pattern repeats every 1024 bytes of
+// shared-memory address, and the consumers' addressing assumes it starts at each buffer).
 template <int KW, int S, class Body, class SW = QsvSweep>
 __host__ __device__ constexpr size_t sweep_smem_bytes() {
     return ((size_t)S << KW) * sizeof(typename Body::Amp) +
-           (Body::kSmemOps ? sizeof(typename SW::op_type) * QSV_MAX_SWEEP_OPS : 0);
+           (Body::kSmemOps ? sizeof(typename SW::op_type) * QSV_MAX_SWEEP_OPS : 0) + QSV_SMEM_ALIGN;
 }
 
 // The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S, Body, SW>() bytes
@@ -92,10 +94,12 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
     constexpr uint32_t TILE_BYTES = (uint32_t)TILE * (uint32_t)sizeof(Amp);
     static_assert(Body::kHalfBits + 3 + 2 + RB + WB == KW, "layout must cover the window");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    Amp *bufs = reinterpret_cast<Amp *>(smem_raw);
+    static_assert(QSV_SMEM_ALIGN == 1024, "the 128-byte swizzle repeats every 1024 bytes");
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    Amp *bufs = reinterpret_cast<Amp *>(smem);
     // the interpreter's op table, copied once from the parameter block: shared-memory reads of an op's
     // fields are independent short-latency loads (the constant-bank path serialises run-time indices)
-    Op *sops = reinterpret_cast<Op *>(smem_raw + ((size_t)S << KW) * sizeof(Amp));
+    Op *sops = reinterpret_cast<Op *>(smem + ((size_t)S << KW) * sizeof(Amp));
     // full barrier of tile j: full[j % (S * G)]. Tiles sharing a full barrier share a buffer (j % S) and a
     // consumer group (j % G), so each full barrier is waited on by one group, phase after phase (a parity
     // wait never meets a phase two steps old). done[b] is waited on by the producer alone, tile by tile.

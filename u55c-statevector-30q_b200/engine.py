@@ -241,14 +241,16 @@ def _parse_plan(w, n):
         tfree = [int(x) for x in w[pos + 1:pos + 1 + rank]]
         tbox = [int(x) for x in w[pos + 6:pos + 6 + rank]]
         pos += 11
-        nph, nops = int(w[pos]), int(w[pos + 1])
-        pos += 2
+        swz = int(w[pos])
+        nph, nops = int(w[pos + 1]), int(w[pos + 2])
+        pos += 3
         phases = []
         for _ in range(nph):
-            rec = [int(x) for x in w[pos:pos + 12]]
-            pos += 12
+            rec = [int(x) for x in w[pos:pos + 15]]
+            pos += 15
             phases.append(dict(reg_bits=[r for r in rec[:4] if r >= 0], lane_bits=rec[4:6],
-                               warp_bits=[r for r in rec[6:10] if r >= 0], op_begin=rec[10], op_end=rec[11]))
+                               warp_bits=[r for r in rec[6:10] if r >= 0], op_begin=rec[10], op_end=rec[11],
+                               lane_lo=rec[12:15]))
         ops = []
         for _ in range(nops):
             tbit, slot, cmask, c0, c1, kind, cls, cm_reg, cm_c, cm_thr, variant = (int(x) for x in w[pos:pos + 11])
@@ -257,7 +259,7 @@ def _parse_plan(w, n):
             ops.append(dict(tbit=tbit, slot=slot, cmask=cmask & 0xFFFFFFFF, cls0=c0, cls1=c1, kind=kind, cls=cls,
                             cm_reg=cm_reg, cm_c=cm_c, cm_thr=cm_thr & 0xFFFFFFFF, variant=variant, m0=m[:8], m1=m[8:]))
         sweeps.append(dict(kw=kw, lo=lo, H=H, window=list(range(lo)) + H, phases=phases, ops=ops,
-                           tma_rank=rank, tdim_free=tfree, tdim_box=tbox))
+                           tma_rank=rank, tdim_free=tfree, tdim_box=tbox, swizzled=bool(swz)))
     return sweeps
 
 
