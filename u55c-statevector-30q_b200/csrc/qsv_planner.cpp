@@ -421,10 +421,15 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
     if (!C128 && swizzle_enabled()) {
         uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
         const int r = tma_dims(sw, tfree, tbox, tstart, true);
+        // QSV_PHASE_COST overrides the weight of a phase change (tuning studies)
+        static const int phase_cost = [] {
+            const char *e = std::getenv("QSV_PHASE_COST");
+            return e ? std::atoi(e) : 2;
+        }();
         auto cost = [](const std::vector<OpT> &o, const std::vector<QsvPhaseX> &p) {
             int lane = 0;
             for (const OpT &x : o) lane += x.slot >= QSV_SLOT_LANE0 && x.variant != QSV_V_SKIP;
-            return lane + 2 * ((int)p.size() - 1);
+            return lane + phase_cost * ((int)p.size() - 1);
         };
         // phases with fewer shuffle ops but more round trips, or the reverse: try lane-op budgets per phase
         for (int cap : {0, 1, 2, 8}) {
