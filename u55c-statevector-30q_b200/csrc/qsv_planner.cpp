@@ -202,20 +202,12 @@ static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart
 // swz (complex64 only): the swizzled layout, in which lane bit l (0-2) sits on tile bit 1+l or 4+l, chosen
 // per phase, so tile bits 1-3 need slots like the others and can be register bits; lane_cap bounds its
 // lane-bit targets (warp-shuffle ops) per phase.
+// Ops [b, e) in tile coordinates with their matrix classes, kinds and code variants (layout-independent).
 template <class OpT>
-static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n, int kw,
-                       std::vector<OpT> &out, std::vector<QsvPhaseX> &phases, std::string &err, bool swz = false,
-                       int lane_cap = 8) {
+static void classify_ops(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n,
+                         std::vector<OpT> &out) {
     constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
-    constexpr int FIXED_LO = C128 ? 0 : 1;       // first tile bit on lane bits 0-2
-    constexpr int FREE_LO = FIXED_LO + 3;        // tile bits from here on need a slot when targeted
-    int rb, wb;
-    if (C128 ? layout_for_kw_c128(kw, &rb, &wb) : layout_for_kw(kw, &rb, &wb)) {
-        err = "unsupported window size";
-        return QSV_ERR_UNSUPPORTED;
-    }
     out.assign(e - b, OpT());
-    phases.clear();
     for (size_t i = b; i < e; i++) {
         OpT &o = out[i - b];
         std::memset(&o, 0, sizeof(o));
@@ -252,6 +244,21 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
             o.variant = QSV_V_MUX;
         }
     }
+}
+
+// The phases of classified ops (their slots and layout-dependent fields are set here).
+template <class OpT>
+static int plan_phases(std::vector<OpT> &out, int kw, std::vector<QsvPhaseX> &phases, std::string &err,
+                       bool swz, int lane_cap) {
+    constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
+    constexpr int FIXED_LO = C128 ? 0 : 1;       // first tile bit on lane bits 0-2
+    constexpr int FREE_LO = FIXED_LO + 3;        // tile bits from here on need a slot when targeted
+    int rb, wb;
+    if (C128 ? layout_for_kw_c128(kw, &rb, &wb) : layout_for_kw(kw, &rb, &wb)) {
+        err = "unsupported window size";
+        return QSV_ERR_UNSUPPORTED;
+    }
+    phases.clear();
     if (C128) swz = false;
     const size_t nops = out.size();
     // swizzled layout: tile bits 1+l and 4+l pair up on lane bit l
@@ -384,6 +391,14 @@ static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const
 }
 
 template <class OpT>
+static int plan_window(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n, int kw,
+                       std::vector<OpT> &out, std::vector<QsvPhaseX> &phases, std::string &err, bool swz = false,
+                       int lane_cap = 8) {
+    classify_ops<OpT>(ops, b, e, tile_of, n, out);
+    return plan_phases<OpT>(out, kw, phases, err, swz, lane_cap);
+}
+
+template <class OpT>
 static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64_t qset, int n, int kw,
                       QsvSweepT<OpT> &sw, std::string &err) {
     constexpr bool C128 = std::is_same<OpT, QsvOpD>::value;
@@ -412,13 +427,17 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         sw.tma_rank = (uint8_t)r;
         for (int d = 0; d < r; d++) { sw.tdim_free[d] = tfree[d]; sw.tdim_box[d] = tbox[d]; }
     }
-    std::vector<OpT> vops;
+    std::vector<OpT> base, vops;
     std::vector<QsvPhaseX> vph;
-    int rc = plan_window<OpT>(ops, b, e, tile_of, n, kw, vops, vph, err);
+    classify_ops<OpT>(ops, b, e, tile_of, n, base);
+    vops = base;
+    int rc = plan_phases<OpT>(vops, kw, vph, err, false, 8);
     if (rc) return rc;
     // the swizzled layout where it costs less: cost = lane ops + 2 per phase change (a shared-memory round
     // trip moves as many bytes through the shared-memory pipe as two shuffle ops); ties keep the plain one
-    if (!C128 && swizzle_enabled()) {
+    int plain_lane = 0;
+    for (const OpT &x : vops) plain_lane += x.slot >= QSV_SLOT_LANE0 && x.variant != QSV_V_SKIP;
+    if (!C128 && swizzle_enabled() && plain_lane > 0) {
         uint8_t tfree[QSV_TMA_MAX_RANK], tbox[QSV_TMA_MAX_RANK], tstart[QSV_TMA_MAX_RANK];
         const int r = tma_dims(sw, tfree, tbox, tstart, true);
         // QSV_PHASE_COST overrides the weight of a phase change (tuning studies)
@@ -433,10 +452,11 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
         };
         // phases with fewer shuffle ops but more round trips, or the reverse: try lane-op budgets per phase
         for (int cap : {0, 1, 2, 8}) {
-            std::vector<OpT> sops;
+            if (!r) break;
+            std::vector<OpT> sops = base;
             std::vector<QsvPhaseX> sph;
             std::string serr;
-            if (r && plan_window<OpT>(ops, b, e, tile_of, n, kw, sops, sph, serr, true, cap) == QSV_OK &&
+            if (plan_phases<OpT>(sops, kw, sph, serr, true, cap) == QSV_OK &&
                 sph.size() <= QSV_MAX_PHASES && cost(sops, sph) < cost(vops, vph)) {
                 vops.swap(sops);
                 vph.swap(sph);
