@@ -86,24 +86,43 @@ def controlled_target(M, nq):
     return None
 
 
-def ops_2q(M, a, b, stats):
-    """4x4 gate on storage qubits (a, b), basis bit_a + 2*bit_b -> MUX2 ops (compiler.py:78-92):
-    diagonal -> one MUX2 on b selected by a; controlled-U -> one MUX2; otherwise the cosine-sine
-    decomposition into three MUX2 (block-diag on a | rotation on b | block-diag on a)."""
+def _ops_2q_records(M):
+    """The MUX2 records of a 4x4 gate, independent of its qubits: ([(target_is_a, M0, M1), ...], csd)."""
     d = np.diag(M)
     if not np.any(np.abs(M - np.diag(d)) > 1e-12):      # np.allclose(M, diag(M), atol=1e-12)
-        return [Op(b, (a,), np.diag([d[0], d[2]]), np.diag([d[1], d[3]]))]
+        return [(False, np.diag([d[0], d[2]]), np.diag([d[1], d[3]]))], False
     ct = controlled_target(M, 2)
     if ct is not None:
         j, U = ct
-        tgt, ctl = (a, b) if j == 0 else (b, a)
-        return [Op(tgt, (ctl,), I2, U)]
+        return [(j == 0, I2, U)], False
     (u1, u2), theta, (v1h, v2h) = cossin(M, p=2, q=2, separate=True)
     c, s = np.cos(theta), np.sin(theta)
     R0 = np.array([[c[0], -s[0]], [s[0], c[0]]])
     R1 = np.array([[c[1], -s[1]], [s[1], c[1]]])
-    stats.csd_2q += 1
-    return [Op(a, (b,), v1h, v2h), Op(b, (a,), R0, R1), Op(a, (b,), u1, u2)]
+    return [(True, v1h, v2h), (False, R0, R1), (True, u1, u2)], True
+
+
+# records of recently seen 4x4 matrices (CX / CZ and other fixed gates repeat in every layer); the
+# matrices are shared between ops and never modified in place
+_OPS_2Q_CACHE = {}
+
+
+def ops_2q(M, a, b, stats):
+    """4x4 gate on storage qubits (a, b), basis bit_a + 2*bit_b -> MUX2 ops (compiler.py:78-92):
+    diagonal -> one MUX2 on b selected by a; controlled-U -> one MUX2; otherwise the cosine-sine
+    decomposition into three MUX2 (block-diag on a | rotation on b | block-diag on a)."""
+    M = np.asarray(M)
+    key = (M.dtype.str, M.shape, M.tobytes())
+    hit = _OPS_2Q_CACHE.get(key)
+    if hit is None:
+        hit = _ops_2q_records(M)
+        if len(_OPS_2Q_CACHE) >= 4096:
+            _OPS_2Q_CACHE.clear()
+        _OPS_2Q_CACHE[key] = hit
+    recs, csd = hit
+    if csd:
+        stats.csd_2q += 1
+    return [Op(a, (b,), m0, m1) if ta else Op(b, (a,), m0, m1) for ta, m0, m1 in recs]
 
 
 def _lower(name, nq, params):
@@ -208,6 +227,19 @@ def pass_window(qubits, k, max_high=MAX_HIGH):
     return None
 
 
+def _fits(hi, k, M):
+    """pass_window(...) is not None for a pass whose qubits at or above k - M are the sorted list hi."""
+    for m in range(M + 1):
+        lim = k - m
+        c = 0
+        for q in hi:
+            if q >= lim:
+                c += 1
+        if c <= m:
+            return True
+    return False
+
+
 def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=MAX_HIGH):
     """Greedy pass packing with remap insertion (compiler.py:186-260).
 
@@ -221,13 +253,14 @@ def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=
     k = min(k, L)
     steps = []
     seg = []
-    cur, cur_set = [], set()
+    lim = k - M                       # only qubits from here on decide whether a pass window fits
+    cur, cur_hi = [], set()
 
     def close_pass():
-        nonlocal cur, cur_set
+        nonlocal cur, cur_hi
         if cur:
             seg.append(cur)
-        cur, cur_set = [], set()
+        cur, cur_hi = [], set()
 
     def close_segment():
         close_pass()
@@ -244,7 +277,8 @@ def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=
 
     for idx, op in enumerate(ops):
         phys = [l2p[q] for q in op.q]
-        if any(p >= L for p in phys) or pass_window(set(phys), k, M) is None:
+        hi_new = [p for p in phys if p >= lim]    # qubits below k - M always fit (and are below L)
+        if hi_new and (any(p >= L for p in hi_new) or not _fits(sorted(set(hi_new)), k, M)):
             low = k - M
             assert len(phys) <= low + M, "op wider than the tile window"
             by_far = lambda p: -next_use(p, idx)          # noqa: E731  furthest next use first
@@ -277,12 +311,17 @@ def schedule(ops, n, L, k, stats, remap_policy="lru", tiling=True, l2p0=None, M=
             new_of_old = {old: new for new, old in enumerate(perm)}
             l2p = [new_of_old[p] for p in l2p]
             phys = [l2p[q] for q in op.q]
-        grown = cur_set | set(phys)
-        if (not tiling and cur) or len(cur) >= MAX_OPS_PER_PASS or pass_window(grown, k, M) is None:
+            hi_new = [p for p in phys if p >= lim]
+        if hi_new:
+            grown = cur_hi.union(hi_new)
+            widened = len(grown) > len(cur_hi)
+        else:
+            grown, widened = cur_hi, False
+        if (not tiling and cur) or len(cur) >= MAX_OPS_PER_PASS or (widened and not _fits(sorted(grown), k, M)):
             close_pass()
-            grown = set(phys)
+            grown = set(hi_new)
         cur.append((op, phys))
-        cur_set = grown
+        cur_hi = grown
     close_segment()
     return steps, l2p
 
@@ -294,7 +333,7 @@ def encode_segment(passes, L, k, M=MAX_HIGH, dtype="c64"):
     c128 = dtype == "c128"
     if dtype not in ("c64", "c128"):
         raise ValueError(f"dtype must be 'c64' or 'c128', not {dtype!r}")
-    words = [MAGIC, L, len(passes), k, DTYPE_C128 if c128 else DTYPE_C64, 0, 0, 0]
+    parts = [np.array([MAGIC, L, len(passes), k, DTYPE_C128 if c128 else DTYPE_C64, 0, 0, 0], dtype=np.int32)]
     for p in passes:
         qubits = set(q for _, ph in p for q in ph)
         m, hi = pass_window(qubits, k, M)
@@ -302,31 +341,33 @@ def encode_segment(passes, L, k, M=MAX_HIGH, dtype="c64"):
         tile_of = {q: q for q in qubits if q < k - m}
         for i, q in enumerate(hi):
             tile_of[q] = k - m + i
-        words += [m, slots[0], slots[1], len(p), slots[2], slots[3], 0, 0]
+        nops = len(p)
+        parts.append(np.array([m, slots[0], slots[1], nops, slots[2], slots[3], 0, 0], dtype=np.int32))
         # op records: matrices rounded to complex64 together (same per-entry rounding as one by one)
-        mats = np.empty((len(p), 2, 4), dtype=np.complex128)
-        for j, (op, ph) in enumerate(p):
-            mats[j, 0] = np.asarray(op.M0, dtype=complex).reshape(-1)
-            mats[j, 1] = np.asarray(op.M1, dtype=complex).reshape(-1)
+        mats = np.empty((nops, 2, 4), dtype=np.complex128)
+        mats[:, 0] = np.array([op.M0 for op, _ in p], dtype=complex).reshape(nops, 4)
+        mats[:, 1] = np.array([op.M1 for op, _ in p], dtype=complex).reshape(nops, 4)
         if c128:
-            fl = np.empty((len(p), 16), dtype=np.float64)
+            fl = np.empty((nops, 16), dtype=np.float64)
             fl[:, 0:8:2], fl[:, 1:8:2] = mats[:, 0].real, mats[:, 0].imag
             fl[:, 8:16:2], fl[:, 9:16:2] = mats[:, 1].real, mats[:, 1].imag
         else:
             c64 = mats.astype(np.complex64)
-            fl = np.empty((len(p), 16), dtype=np.float32)
+            fl = np.empty((nops, 16), dtype=np.float32)
             fl[:, 0:8:2], fl[:, 1:8:2] = c64[:, 0].real, c64[:, 0].imag
             fl[:, 8:16:2], fl[:, 9:16:2] = c64[:, 1].real, c64[:, 1].imag
         fbits = np.ascontiguousarray(fl).view(np.int32)
+        rec = np.zeros((nops, 8 + fbits.shape[1]), dtype=np.int32)
+        rec[:, 0] = OP_MUX2
         for j, (op, ph) in enumerate(p):
-            tq = [tile_of[q] for q in ph]
             cmask = 0
-            for c in tq[1:]:
-                cmask |= 1 << c
-            words += [OP_MUX2, tq[0], cmask, 0, 0, 0, 0, 0]
-            words += fbits[j].tolist()
-    arr = np.asarray(words, dtype=np.int64)
-    return (arr & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
+            for c in ph[1:]:
+                cmask |= 1 << tile_of[c]
+            rec[j, 1] = tile_of[ph[0]]
+            rec[j, 2] = cmask
+        rec[:, 8:] = fbits
+        parts.append(rec.reshape(-1))
+    return np.concatenate(parts)
 
 
 def segment_dtype(seg):
