@@ -59,3 +59,22 @@ def test_budget_limits_resident_memory(torch):
     assert len(done) == 10 and srv.stats["peak_bytes"] <= budget and srv.used == 0
     with pytest.raises(MemoryError):
         Server(budget_bytes=Server.footprint(16) - 1).run([Request(0, gen.random_layer(16, 2, 0), 0.0)])
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("policy", ["sjf", "fifo"])
+def test_compile_on_arrival_equals_plain(torch, policy):
+    """Programs compiled as requests arrive, in a pool of worker processes started before the arrivals
+    (shortest-work-first takes each finished compilation at once; FIFO keeps arrival order): every
+    result equals the plain path's, which compiles in line."""
+    srv = Server(budget_bytes=2e9, max_inflight=6, compile_workers=2, policy=policy)
+    try:
+        srv.warm()
+        done = srv.run(_requests(24, 3000.0, 7))
+    finally:
+        srv.close()
+    assert len(done) == 24 and engine.device_status() == 0
+    alone = {r.rid: r for r in plain_serve(_requests(24, 1e9, 7))}
+    for r in done:
+        a = alone[r.rid]
+        assert r.result[0] == a.result[0] and np.array_equal(r.result[1], a.result[1])

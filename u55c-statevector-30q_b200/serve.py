@@ -94,6 +94,13 @@ def _compile_request(payload):
     return [s for _, s in prog], fmap, m, n
 
 
+def _warm_worker(i):
+    """Compile a small circuit in a worker process (imports and first-use costs paid before serving)."""
+    from .generators import random_layer
+    compile_circuit(random_layer(12, 2, i), 12, 12)
+    return i
+
+
 class _ReadyQueue:
     """Requests whose program exists, waiting for admission. policy "sjf": smallest estimated work first,
     except that a request waiting longer than max_wait seconds goes first (no starvation); "fifo": arrival
@@ -145,10 +152,17 @@ class Server:
         self.policy, self.max_wait = policy, max_wait
         self.stats = dict(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0)
         self.pool = None
+        self.compile_workers = compile_workers
         if compile_workers:
             import multiprocessing as mp
             from .batch import _boot_code
             self.pool = mp.get_context("spawn").Pool(compile_workers, initializer=exec, initargs=(_boot_code(),))
+
+    def warm(self):
+        """Start the compile workers (interpreter start, imports, one small compilation each) and wait for
+        them: a long-running service does this once at start-up, not while requests wait."""
+        if self.pool is not None:
+            self.pool.map(_warm_worker, range(self.compile_workers), chunksize=1)
 
     def close(self):
         if self.pool is not None:
@@ -235,10 +249,22 @@ class Server:
                     compiling.append((r, self.pool.apply_async(_compile_request, ((r.circuit, r.spec, self.k),))))
                 if self.pool is None and realtime:
                     break                 # compile inline one at a time, keep the device fed meanwhile
-            while compiling and compiling[0][1].ready():
-                r, fut = compiling.popleft()
-                self._finish_compile(r, fut.get())
-                ready.append(r)
+            if self.policy == "fifo":
+                while compiling and compiling[0][1].ready():      # arrival order
+                    r, fut = compiling.popleft()
+                    self._finish_compile(r, fut.get())
+                    ready.append(r)
+            elif compiling:
+                # shortest-work-first: every finished compilation joins the ready queue at once (a long
+                # compilation ahead of it does not hold it back)
+                still = deque()
+                for r, fut in compiling:
+                    if fut.ready():
+                        self._finish_compile(r, fut.get())
+                        ready.append(r)
+                    else:
+                        still.append((r, fut))
+                compiling = still
             # admission: free slot and memory budget; continuous -- new work joins while old runs
             admit = []
             streams_left = len(self.free_streams)
