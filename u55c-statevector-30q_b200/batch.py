@@ -33,8 +33,44 @@ def _compile_one(args):
     return prog, fmap, n, stats.n_passes
 
 
-def compile_many(circuits, k=12, workers=0, timeout=600):
-    """Compile circuits to QSV2 programs, in `workers` spawned processes (0 = in this process)."""
+def _warm_one(i):
+    """A small compilation in a worker process (imports and first-use costs paid at pool start-up)."""
+    from .generators import random_layer
+    compile_circuit(random_layer(12, 2, i), 12, 12)
+    return i
+
+
+class CompilePool:
+    """A persistent pool of spawned compile workers: started (and warmed) once, then used for batch after
+    batch, as a service keeps its workers. Use as a context manager or close() it."""
+
+    def __init__(self, workers):
+        import multiprocessing as mp
+        self.workers = max(1, int(workers))
+        self.pool = mp.get_context("spawn").Pool(self.workers, initializer=exec, initargs=(_boot_code(),))
+        self.pool.map(_warm_one, range(self.workers), chunksize=1)
+
+    def compile(self, circuits, k=12, timeout=600):
+        jobs = [(qc, qc.num_qubits if qc.num_qubits <= SMALL_MAX else k) for qc in circuits]
+        return self.pool.map_async(_compile_one, jobs, chunksize=max(1, len(jobs) // (4 * self.workers))).get(timeout)
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.terminate()
+            self.pool = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def compile_many(circuits, k=12, workers=0, timeout=600, pool=None):
+    """Compile circuits to QSV2 programs: in a CompilePool when one is given, else in `workers` spawned
+    processes started for this call (0 = in this process)."""
+    if pool is not None:
+        return pool.compile(circuits, k, timeout)
     jobs = [(qc, qc.num_qubits if qc.num_qubits <= SMALL_MAX else k) for qc in circuits]
     if workers and len(jobs) > 1:
         import multiprocessing as mp

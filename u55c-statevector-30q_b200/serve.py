@@ -94,13 +94,6 @@ def _compile_request(payload):
     return [s for _, s in prog], fmap, m, n
 
 
-def _warm_worker(i):
-    """Compile a small circuit in a worker process (imports and first-use costs paid before serving)."""
-    from .generators import random_layer
-    compile_circuit(random_layer(12, 2, i), 12, 12)
-    return i
-
-
 class _ReadyQueue:
     """Requests whose program exists, waiting for admission. policy "sjf": smallest estimated work first,
     except that a request waiting longer than max_wait seconds goes first (no starvation); "fifo": arrival
@@ -162,7 +155,8 @@ class Server:
         """Start the compile workers (interpreter start, imports, one small compilation each) and wait for
         them: a long-running service does this once at start-up, not while requests wait."""
         if self.pool is not None:
-            self.pool.map(_warm_worker, range(self.compile_workers), chunksize=1)
+            from .batch import _warm_one
+            self.pool.map(_warm_one, range(self.compile_workers), chunksize=1)
 
     def close(self):
         if self.pool is not None:
