@@ -195,14 +195,8 @@ static int tma_dims(const SW &sw, uint8_t *tfree, uint8_t *tbox, uint8_t *tstart
     return rank;
 }
 
-// Ops [b, e) in tile coordinates of a window (tile_of[q] = tile bit of physical qubit q) and their phases.
-// Phases are greedy in op order: tile bits above the fixed lane bits (>= 4 for complex64, whose tile bit 0
-// is the packed half of a float4 and bits 1-3 are lanes; >= 3 for complex128, bits 0-2 lanes) that are
-// targets need a register or lane slot.
-// swz (complex64 only): the swizzled layout, in which lane bit l (0-2) sits on tile bit 1+l or 4+l, chosen
-// per phase, so tile bits 1-3 need slots like the others and can be register bits; lane_cap bounds its
-// lane-bit targets (warp-shuffle ops) per phase.
-// Ops [b, e) in tile coordinates with their matrix classes, kinds and code variants (layout-independent).
+// Ops [b, e) in tile coordinates of a window (tile_of[q] = tile bit of physical qubit q) with their matrix
+// classes, kinds and code variants (independent of the thread layout).
 template <class OpT>
 static void classify_ops(const std::vector<PhysOp> &ops, size_t b, size_t e, const int *tile_of, int n,
                          std::vector<OpT> &out) {
@@ -246,7 +240,12 @@ static void classify_ops(const std::vector<PhysOp> &ops, size_t b, size_t e, con
     }
 }
 
-// The phases of classified ops (their slots and layout-dependent fields are set here).
+// The phases of classified ops, greedy in op order, and each op's slot and layout-dependent fields. Plain
+// layout: tile bits above the fixed lane bits (>= 4 for complex64, whose tile bit 0 is the packed half of a
+// float4 and bits 1-3 are lanes; >= 3 for complex128, bits 0-2 lanes) that are targets need a register or
+// lane slot. swz (complex64 only): the swizzled layout, in which lane bit l (0-2) sits on tile bit 1+l or
+// 4+l, chosen per phase, so tile bits 1-3 need slots like the others and can be register bits; lane_cap
+// bounds its lane-bit targets (warp-shuffle ops) per phase.
 template <class OpT>
 static int plan_phases(std::vector<OpT> &out, int kw, std::vector<QsvPhaseX> &phases, std::string &err,
                        bool swz, int lane_cap) {
