@@ -51,10 +51,12 @@ constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
 
 // Consumer groups per CTA for a sweep. Two groups (16 consumer warps taking alternate tiles, registers
-// capped near 96 per thread) hide the phase round trips of light 13-qubit sweeps; sweeps with many dense
-// or warp-shuffle ops are FP32-bound and run faster with one group and more registers (measured on the
-// 30-qubit random-layer program: 3.05 -> 2.96 ms for 7-8 dense ops, 4.4 -> 5.3 ms for 12).
-// QSV_JIT_GROUPS13=1 or 2 forces one choice.
+// capped at 96 per thread: 17 warps share the four schedulers' register files) overlap one group's phase
+// round trips with the other's arithmetic. Warp-shuffle ops need the most registers: with more than three
+// the kernel spills, so it takes one group. Measured on the 30-qubit random-layer program: 3.05 -> 2.96 ms
+// for sweeps with 7-8 dense ops; with swizzled layouts, 4.65-4.69 -> 4.46-4.53 ms for the FP32-bound
+// sweeps with 12 dense ops and 0-3 shuffle ops (before swizzled layouts those had 5-6 shuffle ops and ran
+// slower with two groups, 4.4 -> 5.3 ms). QSV_JIT_GROUPS13=1 or 2 forces one choice.
 int groups_for(const QsvSweep &sw, int wb) {
     static const int forced = [] {
         const char *e = std::getenv("QSV_JIT_GROUPS13");
@@ -62,15 +64,12 @@ int groups_for(const QsvSweep &sw, int wb) {
     }();
     if (sw.kw != 13 || wb > 3) return 1;
     if (forced == 1 || forced == 2) return forced;
-    int dense = 0, lane = 0;
+    int lane = 0;
     for (int o = 0; o < sw.nops; o++) {
         const QsvOp &op = sw.ops[o];
-        const int v = op.variant;
-        dense += v == QSV_V_UNI_DENSE || v == QSV_V_CTRL_DENSE || v == QSV_V_CTRL_DENSE_SEL ||
-                 (v == QSV_V_MUX && op.cls1 == QSV_M_DENSE) || op.slot == QSV_SLOT_COMP;
-        lane += op.slot >= QSV_SLOT_LANE0 && v != QSV_V_SKIP;
+        lane += op.slot >= QSV_SLOT_LANE0 && op.variant != QSV_V_SKIP;
     }
-    return dense <= 8 && lane <= 2 ? 2 : 1;
+    return lane <= 3 ? 2 : 1;
 }
 
 // Whether a sweep's kernel interleaves the phases of two tiles per consumer thread (sweep_pipeline IL).
