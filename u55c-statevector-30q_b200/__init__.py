@@ -9,6 +9,7 @@ Layers (host side in Python, device side in ``csrc/``):
   runtime    SVRuntime, the drop-in for the reference's XRT runtime
   batch      many circuits per persistent launch, CUDA-graph replay, tile autotuner
   serve      continuous-batching server with HBM-budget admission
+  sharded    one state over several GPUs (one process per GPU, NCCL exchanges of half slices)
 """
 from . import isa, gates, circuit, generators, compiler, qasm  # noqa: F401
 from .circuit import Circuit  # noqa: F401
