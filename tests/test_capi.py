@@ -157,3 +157,16 @@ def test_no_gpu_calls_fail_loudly(lib):
         pytest.skip("GPU present")
     with pytest.raises(RuntimeError):
         engine.new_state(12)
+
+
+def test_swizzled_plans_remove_shuffles(lib):
+    """RL-30: most sweeps take the swizzled layout, and the ones over qubits 0-12 (12-13 dense ops) keep at
+    most three warp-shuffle ops (with lane bits fixed on tile bits 1-3 they had five or six)."""
+    prog, fmap, st = q.compile_circuit(gen.random_layer(30, 24, 1), 30, 12)
+    plan = engine.plan_segment(prog[0][1], 30)
+    assert len(plan) == 84
+    assert sum(sw["swizzled"] for sw in plan) >= 60
+    for sw in plan:
+        if sw["lo"] >= 9 and len(sw["ops"]) >= 12:
+            shuffles = sum(1 for o in sw["ops"] if o["slot"] >= 8 and o["variant"] != 0)
+            assert sw["swizzled"] and shuffles <= 3, (sw["lo"], shuffles)
