@@ -51,7 +51,7 @@ extern "C" {
 #define QSV_C128 1                 /* complex128 amplitudes (QSV2 with FP64 matrices, header word 4 = 1;
                                       an extension with no reference counterpart: the FPGA engine is
                                       complex64 only). Accepted by run_segment, remap, zero_state,
-                                      reduce_f64, chunk_probs_f64 and sample_f64. */
+                                      reduce_f64, reduce_f64_noalloc, chunk_probs_f64 and sample_f64. */
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 QSV_API int qsv_version(void);
@@ -84,17 +84,19 @@ QSV_API size_t qsv_reduce_scratch_bytes(int n);
 QSV_API int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *scratch, size_t scratch_bytes,
                    void *stream);
 
-/* The same FP64 reductions as qsv_reduce_f64, for callers that cannot allocate device memory: code that
- * runs where the device heap belongs to another allocator, or that must keep a fixed footprint once it is
- * running (a long-lived service), or that reaches this library through an FFI with no CUDA allocator of
- * its own. No counterpart in the reference. It takes no scratch argument and allocates nothing: the block
- * partials go to a fixed 256 KiB array compiled into the library (file scope), which every GPU that loads
- * the library holds until the process exits. The array covers every supported size; n outside [10, 34] is
- * rejected with QSV_ERR_INVALID_ARG and a message. The first call on a device looks up the array's device
- * address (once per device, with that device current), so make that first call before any stream capture.
- * All calls share the one array and it keeps the last call's partials; every call overwrites each partial
- * it reads, so nothing needs clearing, but calls whose kernels overlap on the GPU (two streams, two host
- * threads) race on it: order them on one stream or synchronise between them. */
+/* The same FP64 reductions as qsv_reduce_f64 (complex64 or complex128 states), for callers that cannot
+ * allocate device memory: code that runs where the device heap belongs to another allocator, or that must
+ * keep a fixed footprint once it is running (a long-lived service), or that reaches this library through an
+ * FFI with no CUDA allocator of its own. No counterpart in the reference. It takes no scratch argument and
+ * allocates nothing: the block partials go to a fixed 256 KiB array compiled into the library (file scope),
+ * which every GPU that loads the library holds until the process exits. The array covers every supported
+ * size (at most 25,600 doubles, at n = 34); n outside [10, 34] is rejected with QSV_ERR_INVALID_ARG and a
+ * message, a dtype other than QSV_C64 / QSV_C128 with QSV_ERR_UNSUPPORTED. The first call on a device looks
+ * up the array's device address (once per device, with that device current) and caches it, so make that
+ * first call before any stream capture, and do not reset the device (cudaDeviceReset) while the library is
+ * loaded. All calls share the one array and it keeps the last call's partials; every call overwrites each
+ * partial it reads, so nothing needs clearing, but calls whose kernels overlap on the GPU (two streams, two
+ * host threads) race on it: order them on one stream or synchronise between them. */
 QSV_API int qsv_reduce_f64_noalloc(const void *state, int n, int dtype, double *out_dev, void *stream);
 
 /* Probability of each chunk of 2^chunk_bits consecutive amplitudes, FP64 (2^(n - chunk_bits) doubles).

@@ -324,13 +324,14 @@ cudaError_t launch_set_amp0(void *state, int dtype, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-int reduce_bits(int n) {
+constexpr int reduce_bits_of(int n) {
     int B = n - 10;
     if (B < 13) B = 13;
     if (B > n) B = n;
     if (B > 25) B = 25;
     return B;
 }
+int reduce_bits(int n) { return reduce_bits_of(n); }
 
 size_t reduce_scratch_bytes(int n, int chunk_bits) {
     const int B = reduce_bits(n);
@@ -352,16 +353,29 @@ cudaError_t launch_reduce(const void *state, int n, int dtype, double *out, void
 }
 
 // ---------------------------------------------------------------- reduction without caller scratch
-// Fixed-size scratch for reduce_f64_noalloc: every supported state (n <= 34) needs at most
-// 2^(n-B) * (B+1) <= 1024 * 26 doubles of block partials; the array holds 32768 doubles (256 KiB). It is
-// part of the module image, so every GPU that loads the library keeps it until the process exits.
+// Fixed-size scratch for reduce_f64_noalloc: a 2^n state needs 2^(n-B) * (B+1) doubles of block partials
+// (B = reduce_bits(n)); the largest supported state (n = 34, B = 24) needs 1024 * 25 = 25600. The array
+// holds 32768 doubles (256 KiB). It is part of the module image, so every GPU that loads the library keeps
+// it until the process exits. The partial count does not depend on the amplitude type.
 #define QSV_NOALLOC_REDUCE_DOUBLES 32768
+#define QSV_NOALLOC_N_MIN 10
+#define QSV_NOALLOC_N_MAX 34
 static __device__ __align__(256) double g_noalloc_reduce_scratch[QSV_NOALLOC_REDUCE_DOUBLES];
+
+constexpr long long noalloc_partials(int n) { return (1ll << (n - reduce_bits_of(n))) * (reduce_bits_of(n) + 1); }
+constexpr bool noalloc_fits_every_n() {
+    for (int n = QSV_NOALLOC_N_MIN; n <= QSV_NOALLOC_N_MAX; n++)
+        if (noalloc_partials(n) > QSV_NOALLOC_REDUCE_DOUBLES) return false;
+    return true;
+}
+static_assert(noalloc_fits_every_n(), "the fixed reduction scratch must hold the partials of every supported n");
 
 size_t noalloc_reduce_capacity() { return QSV_NOALLOC_REDUCE_DOUBLES * sizeof(double); }
 
 // Device address of the fixed scratch for the current device. Looked up once per device (the host-side
-// name of the array is only a stand-in for it, never a device address).
+// name of the array is only a stand-in for it, never a device address) and cached for the life of the
+// process: the cache assumes the device's primary context is not reset (cudaDeviceReset) while the library
+// is loaded, since a reset unloads the module and the cached address would then be stale.
 static cudaError_t noalloc_scratch_ptr(double **out) {
     static std::mutex mu;
     static double *ptr[64] = {nullptr};
@@ -380,15 +394,15 @@ static cudaError_t noalloc_scratch_ptr(double **out) {
     return cudaSuccess;
 }
 
-cudaError_t launch_reduce_noalloc(const void *state, int n, double *out, cudaStream_t stream, size_t *need) {
-    const int B = reduce_bits(n);
-    const size_t doubles = ((size_t)1 << (n - B)) * (B + 1);
+cudaError_t launch_reduce_noalloc(const void *state, int n, int dtype, double *out, cudaStream_t stream,
+                                  size_t *need) {
+    const size_t doubles = (size_t)noalloc_partials(n);
     *need = doubles * sizeof(double);
     if (doubles > QSV_NOALLOC_REDUCE_DOUBLES) return cudaErrorInvalidValue;
     double *scratch = nullptr;
     cudaError_t e = noalloc_scratch_ptr(&scratch);
     if (e != cudaSuccess) return e;
-    return launch_reduce(state, n, 0, out, scratch, stream);
+    return launch_reduce(state, n, dtype, out, scratch, stream);
 }
 
 cudaError_t launch_chunk_probs(const void *state, int n, int dtype, int cb, double *out, cudaStream_t stream) {

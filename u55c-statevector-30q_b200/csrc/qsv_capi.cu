@@ -30,7 +30,7 @@ int batch_add(Batch *b, void *state, int n, int nseg, const int32_t *const *segs
 size_t batch_workspace_bytes(Batch *b);
 cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
 cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
-cudaError_t launch_reduce_noalloc(const void *state, int n, double *out, cudaStream_t stream, size_t *need);
+cudaError_t launch_reduce_noalloc(const void *state, int n, int dtype, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
 int jit_set_mode(int mode);
 int jit_prepare(const std::vector<QsvSweep> &sweeps);
@@ -225,11 +225,11 @@ int qsv_reduce_f64(const void *state, int n, int dtype, double *out_dev, void *s
 
 int qsv_reduce_f64_noalloc(const void *state, int n, int dtype, double *out_dev, void *stream) {
     if (!state || !out_dev) return fail(QSV_ERR_INVALID_ARG, "null pointer");
-    if (dtype != QSV_C64) return fail(QSV_ERR_UNSUPPORTED, "only complex64 states are supported");
+    if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");
     if (n < QSV_N_MIN || n > QSV_N_MAX)
         return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34] for the fixed-scratch reduction");
     size_t need = 0;
-    cudaError_t e = qsv::launch_reduce_noalloc(state, n, out_dev, (cudaStream_t)stream, &need);
+    cudaError_t e = qsv::launch_reduce_noalloc(state, n, dtype, out_dev, (cudaStream_t)stream, &need);
     if (need > qsv::noalloc_reduce_capacity())
         return fail(QSV_ERR_SCRATCH, "state needs " + std::to_string(need) + " B of block partials, fixed scratch holds " +
                                          std::to_string(qsv::noalloc_reduce_capacity()) + " B");
