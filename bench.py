@@ -121,6 +121,25 @@ def workload(pkg, n, depth, seed, k=12, max_high=4):
     return qc, prog, fmap, stats
 
 
+def accuracy_vs_fp64(qc):
+    """1 - F and max |delta amp| of the complex64 result of qc against the same circuit run in complex128
+    (FP64 matrices and arithmetic) on the device, from |0...0>, with the reference's recipe
+    (bench/fpga/sv_maxwidth_ref.py:15-25; precision.compare). Both runs use one compiled schedule (same final
+    qubit map), so the states are compared in physical order."""
+    import torch
+    from importlib import import_module
+    precision = import_module("qsv_b200.precision")
+    s128, f128, t128 = precision.run_state(qc, "c128")
+    s64, f64, t64 = precision.run_state(qc, "c64")
+    if f128 != f64:
+        raise RuntimeError("complex64 and complex128 schedules differ")
+    m = precision.compare(s128, s64)
+    del s128, s64
+    torch.cuda.empty_cache()
+    return {"one_minus_f": m["one_minus_f"], "max_abs_err": m["max_abs_err"], "norm": m["norm"],
+            "c128_T_kernel_s": t128["T_kernel"]}
+
+
 # ------------------------------------------------------------------ CPU baseline (golden model)
 def _cpu_worker(args):
     seg, n, tiles, npass = args
@@ -423,6 +442,7 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the complex128 (FP64) comparison runs")
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
                     help="specialised sweep kernels (compiled before the warm-up unless off)")
     ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served", "latency", "families"],
@@ -491,13 +511,13 @@ def main():
     engine = import_module("qsv_b200.engine")
     engine.load()
     sweeps = sum(len(engine.plan_segment(s, a.n)) for s in segs)
-    cfg["sweeps"] = sweeps
+    eng_info = {"sweeps": sweeps}
     engine.set_jit(a.jit)
     if a.jit != "off":
         t0 = time.perf_counter()
         ready = sum(engine.jit_prepare(s, a.n) for s in segs)
-        cfg["specialised_kernels"] = {"sweeps_ready": ready, "structures": engine.jit_info()["structures"],
-                                      "compile_s": round(time.perf_counter() - t0, 2)}
+        eng_info["specialised_kernels"] = {"sweeps_ready": ready, "structures": engine.jit_info()["structures"],
+                                           "compile_s": round(time.perf_counter() - t0, 2)}
     stream = torch.cuda.current_stream(dev)
     state = engine.new_state(a.n, device=dev)
 
@@ -563,9 +583,24 @@ def main():
                "qsv2_passes": qstats.n_passes, "ms_per_step": qsec * 1e3, "value": qgbs, "unit": "GB/s",
                "frac": qgbs / _peaks()[0]}
 
+    # accuracy of every reported result against FP64: the complex64 state of each circuit from |0...0>
+    # against the complex128 engine's state of the same circuit (untimed, after the timed regions)
+    accuracy = None
+    if world == 1 and not a.no_accuracy:
+        del state
+        torch.cuda.empty_cache()
+        accuracy = {"oracle": "complex128 engine on the device (FP64 matrices and arithmetic; value for value "
+                              "equal to the C oracle's FP64 engine in the tests)",
+                    "rl": accuracy_vs_fp64(qc)}
+        if qft is not None:
+            accuracy["qft30"] = accuracy_vs_fp64(pkg.generators.qft(a.n))
+            qft["one_minus_f"] = accuracy["qft30"]["one_minus_f"]
+            qft["max_abs_err"] = accuracy["qft30"]["max_abs_err"]
+        state = engine.new_state(a.n, device=dev)
+
     # live copy-bandwidth probe (the hand-written HBM copy kernel) on the state's size: the achievable
     # ceiling measured in the same process, beside the driver-measured peak used for frac
-    copy_gbs = None
+    copy_gbs = remap = None
     if world == 1:
         dst = torch.empty_like(state)
         for _ in range(2):
@@ -578,6 +613,19 @@ def main():
         c1.record(stream)
         torch.cuda.synchronize(dev)
         copy_gbs = 2 * (8 << a.n) * 5 / (c0.elapsed_time(c1) / 1e3) / 1e9
+        # the remap kernel (replaces sv_swap and the host exchanges): one out-of-place bit permutation of
+        # the whole state, 16 B per amplitude; a permutation that moves low and high qubits
+        perm = [int(x) for x in np.random.default_rng(7).permutation(a.n)]
+        for _ in range(2):
+            engine.remap(state, dst, perm, stream)
+        c0.record(stream)
+        for _ in range(5):
+            engine.remap(state, dst, perm, stream)
+        c1.record(stream)
+        torch.cuda.synchronize(dev)
+        rsec = c0.elapsed_time(c1) / 1e3 / 5
+        remap = {"perm": perm, "ms": rsec * 1e3, "value": (16 << a.n) / rsec / 1e9, "unit": "GB/s",
+                 "frac": (16 << a.n) / rsec / 1e9 / _peaks()[0], "kernel": "qsv::dev::remap_kernel"}
         del dst
 
     # end to end through the public API (host circuit in, sampled counts out)
@@ -611,7 +659,9 @@ def main():
         out = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": sec / a.steps * 1e3, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 arithmetic)",
-               "data": "synthetic (seeded random-layer circuit)", "config": cfg,
+               "data": "synthetic (seeded random-layer circuit)", "config": cfg, "engine": eng_info,
+               "one_minus_f": accuracy["rl"]["one_minus_f"] if accuracy else None,
+               "max_abs_err": accuracy["rl"]["max_abs_err"] if accuracy else None, "accuracy": accuracy,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "peak_kind": peak_kind,
                             "traffic": TRAFFIC_PER_ALGORITHMIC * bytes_per_sweep,
@@ -621,6 +671,7 @@ def main():
                             "algorithmic_bytes_per_launch": bytes_per_sweep,
                             "copy_probe_gbs": copy_gbs},
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "qft30": qft,
+               "remap": remap,
                # the reference's own formula (analysis/make_tables.py:321): QSV2 passes x 16 B x 2^n over
                # the kernel time; above the HBM roofline because consecutive passes share one sweep here
                "reference_formula_gbs": stats.n_passes * bytes_per_sweep * a.steps * world / sec / 1e9}

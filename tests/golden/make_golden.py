@@ -2,7 +2,7 @@
 
 Run once, in a container where the reference tree is present (it is not on GPU hosts):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference root>     (or QSV_REFERENCE_ROOT=<reference root>)
 
 What it runs from the reference (imported from its own files, unmodified):
   * host/sv/compiler.py  compile_circuit / schedule / encode_segment -- with a minimal stand-in for the
@@ -157,4 +157,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QSV_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference root>  (or set QSV_REFERENCE_ROOT)")
+    main(root)

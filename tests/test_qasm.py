@@ -12,7 +12,8 @@ from qsv_b200 import generators as gen
 from qsv_b200.qasm import QasmError, from_qasm, to_qasm
 from oracle import oracle as orc
 
-REF_QASM = "/root/reference/circuits/qasm"
+# the reference's exported circuit files, when a copy of the reference tree is named by QSV_REFERENCE_ROOT
+REF_QASM = os.path.join(os.environ.get("QSV_REFERENCE_ROOT", "-"), "circuits", "qasm")
 
 
 @pytest.mark.parametrize("qc", [gen.qft(10), gen.ghz(12), gen.rqc(10, 6, 3), gen.vqe(11, 2, 4),
