@@ -141,6 +141,18 @@ QSV_API int qsv_hbm_copy(void *dst, const void *src, size_t bytes, void *stream)
  * Synchronous. */
 QSV_API int qsv_device_status(int *status);
 
+/* Failure-detection knob (no reference counterpart): every mbarrier wait of the sweep kernels launched after
+ * this call gives up after `us` microseconds (0 = the default, 2 s), ORs bit 0 into the device status word,
+ * waits (bounded) for its CTA's copies in flight and returns, so a stuck pipeline ends the kernel instead of
+ * hanging the GPU. Process-wide. */
+QSV_API int qsv_set_wait_limit_us(unsigned int us);
+
+/* Fault injection for tests of that path (no reference counterpart): the next `count` sweep launches of
+ * qsv_run_segment have block 0 never issue the load of its first tile, so its waits run out after the wait
+ * limit; the kernel then sets status bit 0 and returns with that block's tiles not updated (the state must
+ * be rebuilt). count 0 disarms it. A host-side switch: no fault, trap or endless wait is involved. */
+QSV_API int qsv_inject_skip_load(int count);
+
 /* Number of kernel launches this thread issued through this library since the last call (and reset
  * the count). No reference counterpart: launch accounting for the benchmark. */
 QSV_API long long qsv_take_launch_count(void);
@@ -156,6 +168,14 @@ QSV_API int qsv_set_layout13(int rb);
 /* Tuning knob (no reference counterpart): how many op targets a phase may place on lane bits (warp
  * shuffles) instead of starting a new phase, 0..2 (default 1). Values are identical either way. */
 QSV_API int qsv_set_phase_lanes(int k);
+
+/* Tuning knob (no reference counterpart): form of the interpreter sweep kernel. 1 (default) = ping-pong:
+ * ops whose code path writes every amplitude a thread holds go from one register set to the other, so the
+ * run-time dispatch of each op leaves no register reconciliation behind, with tiles staged by the consumer
+ * warps themselves (no producer warp, so a thread may hold both register sets); 0 = every op in place,
+ * staged by a producer warp; 2 = every op in place, staged by the consumers. Values are identical in every
+ * form. Returns the previous form, or QSV_ERR_INVALID_ARG. Process-wide. */
+QSV_API int qsv_set_interp_form(int form);
 
 /* Specialised sweep kernels (no reference counterpart; the reference's engine is one fixed HLS kernel).
  * qsv_run_segment can launch, instead of the interpreter kernel, a kernel compiled at run time (NVRTC,

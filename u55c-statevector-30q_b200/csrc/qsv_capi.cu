@@ -1,6 +1,7 @@
 // qsv_capi.cu -- the extern "C" boundary of libqsv_b200.so (declared in include/qsv_b200.h).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -32,6 +33,7 @@ cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
 cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
 cudaError_t launch_reduce_noalloc(const void *state, int n, int dtype, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
+int set_interp_form(int form);
 int jit_set_mode(int mode);
 int jit_prepare(const std::vector<QsvSweep> &sweeps);
 void jit_wait();
@@ -39,6 +41,17 @@ int jit_info(long long *out, int cap);
 std::string jit_last_log();
 int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream, cudaError_t *err);
 }  // namespace qsv
+
+static std::atomic<unsigned> g_wait_us{0};     // bounded-wait limit of the sweep kernels (0: 2 s default)
+static std::atomic<int> g_inject_skip{0};      // fault injection: sweep launches left that skip a tile load
+
+// one armed fault injection, if any (consumed by the launch that takes it)
+static int take_injection() {
+    int c = g_inject_skip.load();
+    while (c > 0 && !g_inject_skip.compare_exchange_weak(c, c - 1)) {
+    }
+    return c > 0 ? 1 : 0;
+}
 
 static thread_local std::string t_err;
 static thread_local long long t_launches = 0;
@@ -93,6 +106,23 @@ int qsv_set_phase_lanes(int k) {
     return QSV_OK;
 }
 
+int qsv_set_wait_limit_us(unsigned int us) {
+    g_wait_us.store(us);
+    return QSV_OK;
+}
+
+int qsv_inject_skip_load(int count) {
+    if (count < 0) return fail(QSV_ERR_INVALID_ARG, "count must be >= 0");
+    g_inject_skip.store(count);
+    return QSV_OK;
+}
+
+int qsv_set_interp_form(int form) {
+    const int old = qsv::set_interp_form(form);
+    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "interpreter form must be 0, 1 or 2");
+    return old;
+}
+
 int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap) {
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     std::vector<qsv::PhysPass> passes;
@@ -121,7 +151,9 @@ int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int d
         rc = qsv::build_sweeps<QsvOpD>(passes, n, kw, g_lo_merge, sweeps, err);
         if (rc) return fail(rc, err);
         std::lock_guard<std::mutex> lk(g_launch_mu);
-        for (const QsvSweepD &sw : sweeps) {
+        for (QsvSweepD &sw : sweeps) {
+            sw.wait_us = g_wait_us.load();
+            sw.skip_load = take_injection();
             cudaError_t e = qsv::launch_sweep_c128((double2 *)state, sw, nsm, (cudaStream_t)stream);
             if (e != cudaSuccess) return cuda_fail(e, "complex128 sweep launch");
             t_launches++;
@@ -133,7 +165,9 @@ int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int d
     rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
     if (rc) return fail(rc, err);
     std::lock_guard<std::mutex> lk(g_launch_mu);
-    for (const QsvSweep &sw : sweeps) {
+    for (QsvSweep &sw : sweeps) {
+        sw.wait_us = g_wait_us.load();
+        sw.skip_load = take_injection();
         cudaError_t e = cudaSuccess;
         const int r = qsv::jit_try_launch((float2 *)state, sw, nsm, (cudaStream_t)stream, &e);
         if (r < 0) return cuda_fail(e, "specialised sweep launch");

@@ -44,21 +44,34 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
-// Bounded wait on an mbarrier phase. Gives up after ~2 s (a sweep tile takes microseconds), records the
-// failure in the device status word and in the CTA's abort flag, and returns false so the caller can
-// leave its loop.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *status) {
+// Bounded wait on an mbarrier phase. Gives up after limit_ns (2 s by default; a sweep tile takes
+// microseconds), records the failure in the device status word and in the CTA's abort flag, and returns
+// false so the caller can leave its loop; a wait that sees another thread's abort returns false as well.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *status,
+                                          uint64_t limit_ns = QSV_WAIT_US_DEFAULT * 1000ull) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort_flag) return false;
-        if (globaltimer_ns() - t0 > 2000000000ull) {
+        if (globaltimer_ns() - t0 > limit_ns) {
             *abort_flag = 1;
             atomicOr(status, 1);
             return false;
         }
     }
+}
+// Bounded wait that ignores the abort flag: after an abort, the thread that issued bulk-async loads waits
+// (at most limit_ns) for the ones still in flight before the CTA exits. Returns whether the phase completed.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    return true;
+}
+// the wait limit a sweep's parameters ask for, in nanoseconds
+__device__ __forceinline__ uint64_t wait_limit_ns(uint32_t wait_us) {
+    return (uint64_t)(wait_us ? wait_us : QSV_WAIT_US_DEFAULT) * 1000ull;
 }
 
 // bulk-async copy global -> shared, completion counted on an mbarrier (bytes)
@@ -76,6 +89,8 @@ __device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, uint32_t 
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// this thread's bulk groups except the most recent one have finished reading their shared-memory source
+__device__ __forceinline__ void bulk_wait_read_but_one() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // make this thread's generic-proxy shared-memory writes visible to the async proxy (bulk stores)
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }

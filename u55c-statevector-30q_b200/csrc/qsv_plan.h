@@ -46,6 +46,7 @@ typedef unsigned long long uint64_t;
 #define QSV_TMA_TENSOR_LO 9     // sub-blocks shorter than 2^9 amplitudes are staged with a tensor-map box
 #define QSV_SMEM_ALIGN 1024     // sweep kernels align their tile buffers to this in dynamic shared memory
 #define QSV_TMA_MAX_RANK 5
+#define QSV_WAIT_US_DEFAULT 2000000u   // bounded mbarrier waits: 2 s (a tile takes microseconds)
 
 // matrix classes (host-detected, exact comparisons). The specialised forms give the same values as the
 // dense fused-multiply-add chain (the skipped terms are exact zeros).
@@ -98,7 +99,8 @@ struct QsvOp {
     uint8_t tbit;               // target tile bit
     uint8_t variant;            // QSV_V_*
     uint8_t r00;                // 1: M0 is dense with m00 real (QSV_M_DENSE_R0 path)
-    uint8_t pad[2];
+    uint8_t oop;                // 1: the op's code path writes every slot (qsv_op_writes_every_slot)
+    uint8_t pad[1];
 };
 
 // complex128 op: the same fields with FP64 matrices. In the complex128 layout tile bits 0-2 are lane bits
@@ -117,8 +119,28 @@ struct QsvOpD {
     uint8_t tbit;
     uint8_t variant;
     uint8_t r00;
-    uint8_t pad[6];
+    uint8_t oop;
+    uint8_t pad[5];
 };
+
+#if defined(__CUDACC__)
+#define QSV_HOST_DEVICE __host__ __device__
+#else
+#define QSV_HOST_DEVICE
+#endif
+
+// Whether an op's code path (complex64 layout) writes every slot a thread holds: the interpreter applies
+// such ops out of place, from one register set into the other (qsv_ops_pp.cuh). Tile-bit-0 targets:
+// uniform dense and diagonal matrices. Register and lane targets: uniform dense / diagonal / swap and the
+// general MUX (every pair computed with per-pair coefficients; on a lane bit unless it is a controlled op
+// with a tile-bit-0 control), and on a register bit the branch-free controlled dense form.
+static inline QSV_HOST_DEVICE bool qsv_op_writes_every_slot(int slot, int variant, int kind, int cls0, int cm_c) {
+    if (variant == QSV_V_SKIP) return false;
+    if (slot == QSV_SLOT_COMP) return kind == QSV_K_UNI && (cls0 == QSV_M_DENSE || cls0 == QSV_M_DIAG);
+    const bool uni = variant == QSV_V_UNI_DENSE || variant == QSV_V_UNI_DIAG || variant == QSV_V_UNI_SWAP;
+    if (slot >= QSV_SLOT_LANE0) return uni || (variant == QSV_V_MUX && !(kind == QSV_K_CTRL && cm_c));
+    return uni || variant == QSV_V_MUX || variant == QSV_V_CTRL_DENSE_SEL;
+}
 
 // A phase's thread layout: lane bits 0-2 sit on tile bits lane_lo[0..2] (1, 2, 3 for complex64 unless the
 // sweep is swizzled, see QsvSweepT::swz; 0, 1, 2 for complex128), lane bits 3-4 on lane_bits[0..1].
@@ -160,6 +182,8 @@ struct QsvSweepT {
     int64_t ntiles;             // 2^(n - kw)
     int32_t nphases;
     int32_t nops;
+    uint32_t wait_us;           // bounded waits give up after this many microseconds (0: QSV_WAIT_US_DEFAULT)
+    int32_t skip_load;          // fault injection for tests: 1 = block 0 never loads its first tile (0: off)
     QsvPhase phases[QSV_MAX_PHASES];
     OpT ops[QSV_MAX_SWEEP_OPS];
 };

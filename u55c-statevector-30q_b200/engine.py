@@ -68,6 +68,9 @@ def load(path=LIB_PATH):
         "qsv_batch_launch": ([P, P, SZ, P], I32),
         "qsv_set_phase_lanes": ([ctypes.c_int], I32),
         "qsv_set_jit": ([ctypes.c_int], I32),
+        "qsv_set_interp_form": ([ctypes.c_int], I32),
+        "qsv_set_wait_limit_us": ([ctypes.c_uint], I32),
+        "qsv_inject_skip_load": ([ctypes.c_int], I32),
         "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
         "qsv_jit_wait": ([], I32),
         "qsv_jit_info": ([P, ctypes.c_int], I32),
@@ -91,7 +94,8 @@ def exported_symbols():
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
             "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
-            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
+            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_interp_form", "qsv_set_wait_limit_us",
+            "qsv_inject_skip_load", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
             "qsv_jit_wait", "qsv_jit_info", "qsv_hbm_copy"]
 
@@ -337,6 +341,26 @@ def hbm_copy(dst, src, stream=None):
 
 
 JIT_MODES = {"off": 0, "eager": 1, "auto": 2}
+
+
+def set_wait_limit_us(us):
+    """Bounded mbarrier waits of the sweep kernels give up after `us` microseconds (0 = default, 2 s)."""
+    _check(load().qsv_set_wait_limit_us(int(us)))
+
+
+def inject_skip_load(count=1):
+    """Fault injection for tests: the next `count` sweep launches have block 0 skip its first tile load, so
+    their bounded waits run out and the device status word records it (0 disarms)."""
+    _check(load().qsv_inject_skip_load(int(count)))
+
+
+def set_interp_form(form):
+    """Interpreter sweep kernel form: 1 = ping-pong register sets (default), 0 = in place with a producer
+    warp, 2 = in place without one. Returns the previous form."""
+    rc = load().qsv_set_interp_form(int(form))
+    if rc < 0:
+        _check(rc)
+    return rc
 
 
 def set_jit(mode):
