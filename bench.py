@@ -281,13 +281,17 @@ def batched_main(a):
 
 
 def served_main(a):
-    """Served: Poisson arrivals (rate per second) of circuits with qubit counts log-uniform in [12, qmax]
-    and depths uniform in [10, 100] (U3 / CZ / Toffoli layers, request i seeded 4 + i), admitted under a
-    160 GB HBM budget with continuous batching, against the plain sequential path on the same requests.
-    Programs are compiled before the run (spawned workers), so both sides time device work and queueing;
-    --compile-on-arrival compiles in a worker pool as requests arrive (the plain path compiles in line).
-    Both sides start warm: the server's compile workers are started and 24 untimed requests of other seeds
-    run through it first (the plain path, timed second in the same process, is warm by then as well)."""
+    """Served (config 5): a Poisson arrival stream of circuits with qubit counts log-uniform in [12, qmax]
+    (default 30) and depths uniform in [10, 100] (U3 / CZ / Toffoli layers, request i seeded 4 + i),
+    admitted under a 160 GB HBM budget (reserved once as the server's arena) with continuous batching, at
+    each arrival rate of --rates (default 50, 200, 500, 1000, 2000 per second), against the plain sequential
+    path (one request at a time, arrival order) on the same requests. Both sides run programs compiled
+    before the run (compilation does not depend on the rate), so neither gains from host compile
+    parallelism; --compile-on-arrival compiles in a warm worker pool on the served side and in line on the
+    plain side instead. --count arrivals per rate (default 20000, the configuration's stream; every rate
+    replays the first --count requests of the same seeded stream, so the requests, and their results, are
+    the same at every rate). Both sides start warm: the server's compile workers are started and 24
+    untimed requests of other seeds run through it first."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     pkg = _package()
@@ -298,47 +302,86 @@ def served_main(a):
     engine.load()
     torch.cuda.set_device(0)
     engine.set_jit(a.jit)
-    count = a.count or 400
+    count = a.count or 20000
+    rates = [float(x) for x in a.rates.split(",")]
     workers = min(16, os.cpu_count() or 1)
-    reqs = serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax)
+    base = serve.config5_requests(count=count, rate=rates[0], qmax=a.qmax)
+    t0 = time.perf_counter()
     if not a.compile_on_arrival:
-        reqs = serve.precompile(reqs, workers=workers)
+        base = serve.precompile(base, workers=workers)
+    t_compile = time.perf_counter() - t0
+    # algorithmic bytes of the whole stream (16 B per amplitude per sweep), from the sweep plans of every
+    # request, or of a uniform sample of 400 of them for longer streams (planning is host work)
+    work_bytes, work_kind = 0, None
+    if not a.compile_on_arrival:
+        sample = base if len(base) <= 2000 else [base[i] for i in np.random.default_rng(0).choice(len(base), 400,
+                                                                                                 replace=False)]
+        work_bytes = sum(sum(len(engine.plan_segment(seg, r.n)) for seg in r.program) * (16 << r.n) for r in sample)
+        work_bytes *= len(base) / len(sample)
+        work_kind = "exact" if len(sample) == len(base) else "estimated from 400 sampled requests"
+
+    def stream(rate):
+        """The same requests (same seeds, same programs) arriving at `rate` per second."""
+        arr = serve.config5_requests(count=count, rate=rate, qmax=a.qmax)
+        out = []
+        for r, b in zip(arr, base):
+            x = serve.Request(b.rid, None, r.arrival, spec=b.spec)
+            if b.program is not None:
+                x.program, x.fmap, x.n, x.n_log, x.work = b.program, b.fmap, b.n, b.n_log, b.work
+            out.append(x)
+        return out
+
     srv = serve.Server(budget_bytes=160e9, max_inflight=16, policy=a.policy,
                        compile_workers=workers if a.compile_on_arrival else 0)
     srv.warm()                      # compile workers started before the arrivals (service start-up)
-    # service warm-up, untimed: a few requests of other seeds through the device (kernel loading,
-    # allocator growth), so neither side of the comparison pays first-use costs inside its timing (the
-    # plain path runs second, in the same process)
-    warm = serve.config5_requests(count=24, rate=1e9, seed=10 ** 6, qmax=a.qmax)
+    warm = serve.config5_requests(count=24, rate=1e9, seed=10 ** 6, qmax=min(a.qmax, 24))
     if not a.compile_on_arrival:
         warm = serve.precompile(warm, workers=workers)
     srv.run(warm)
+    per_rate = []
+    equal_all = True
     with ClockSampler(0) as clk:
-        t = time.perf_counter()
-        done = srv.run(reqs)
-        t_served = time.perf_counter() - t
+        for rate in rates:
+            srv.stats.update(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0,
+                             rejected=0)
+            srv.failed = []
+            t = time.perf_counter()
+            done = srv.run(stream(rate), timeout=7 * 24 * 3600.0)
+            t_served = time.perf_counter() - t
+            st = serve.latency_stats(done)
+            t = time.perf_counter()
+            plain = serve.plain_serve(stream(rate))
+            t_plain = time.perf_counter() - t
+            sp = serve.latency_stats(plain)
+            res = {r.rid: r.result for r in done}
+            equal = len(done) == len(plain) and all(
+                res[r.rid][0] == r.result[0] and np.array_equal(res[r.rid][1], r.result[1]) for r in plain)
+            equal_all = equal_all and equal
+            per_rate.append({"rate_per_s": rate, "served": dict(st, wall_s=t_served, **srv.stats),
+                             "plain": dict(sp, wall_s=t_plain),
+                             "speedup_vs_plain": st["circuits_per_s"] / sp["circuits_per_s"],
+                             "failed": len(srv.failed), "results_identical_alone_and_in_mix": equal})
+            print(json.dumps({"progress": per_rate[-1]}), file=sys.stderr, flush=True)
     srv.close()
-    st = serve.latency_stats(done)
-    reqs2 = serve.config5_requests(count=count, rate=a.rate, qmax=a.qmax)
-    if not a.compile_on_arrival:
-        reqs2 = serve.precompile(reqs2, workers=workers)
-    t = time.perf_counter()
-    plain = serve.plain_serve(reqs2)
-    t_plain = time.perf_counter() - t
-    sp = serve.latency_stats(plain)
-    res = {r.rid: r.result for r in done}
-    equal = all(res[r.rid][0] == r.result[0] and np.array_equal(res[r.rid][1], r.result[1]) for r in plain)
+    top = per_rate[-1]
+    ns = [r.n_log for r in base] if not a.compile_on_arrival else [r.spec[0] for r in base]
     print(json.dumps({"metric": "served circuits/s and p50/p99 latency vs plain sequential",
-                      "value": st["circuits_per_s"], "unit": "circuits/s", "higher_is_better": True,
-                      "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)", "data": "synthetic (seeded requests)",
-                      "config": {"workload": f"{count} Poisson arrivals at {a.rate}/s, n log-uniform in "
-                                             f"[12, {a.qmax}], depth uniform in [10, 100], 160 GB HBM budget",
+                      "value": top["served"]["circuits_per_s"], "unit": f"circuits/s (at {top['rate_per_s']:g}/s)",
+                      "higher_is_better": True, "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)",
+                      "data": "synthetic (seeded requests)",
+                      "config": {"workload": f"{count} Poisson arrivals per rate, rates {a.rates} per second, n "
+                                             f"log-uniform in [12, {a.qmax}], depth uniform in [10, 100], "
+                                             "U3 / CZ brickwork / Toffoli layers, request i seeded 4 + i, 160 GB "
+                                             "HBM budget (reserved arena)",
                                  "admission": a.policy,
                                  "compile": "on arrival (worker pool; plain path in line)" if a.compile_on_arrival
-                                 else "before the run"},
-                      "served": dict(st, wall_s=t_served, **srv.stats), "plain": dict(sp, wall_s=t_plain),
-                      "speedup_vs_plain": st["circuits_per_s"] / sp["circuits_per_s"],
-                      "results_identical_alone_and_in_mix": equal, "clocks": clk.summary()}))
+                                 else "before the run, both sides"},
+                      "qubits": {"min": int(min(ns)), "max": int(max(ns)), "count_30": int(sum(x == 30 for x in ns))},
+                      "algorithmic_bytes": work_bytes or None, "algorithmic_bytes_kind": work_kind,
+                      "hbm_floor_s": (work_bytes / (_peaks()[0] * 1e9)) if work_bytes else None,
+                      "host_compile_s": t_compile, "rates": per_rate,
+                      "speedup_vs_plain": top["speedup_vs_plain"],
+                      "results_identical_alone_and_in_mix": equal_all, "clocks": clk.summary()}))
 
 
 def latency_main(a):
@@ -450,9 +493,9 @@ def main():
                          "(33 qubits complex64, 32 qubits complex128 vs complex64); batched: 512 circuits of "
                          "10..24 qubits per CUDA-graph replay vs one at a time; served: Poisson arrivals of "
                          "12..30-qubit circuits, continuous batching vs the plain sequential path")
-    ap.add_argument("--count", type=int, default=0, help="circuits (batched: 512; served: 400)")
-    ap.add_argument("--rate", type=float, default=2000.0, help="served: arrivals per second")
-    ap.add_argument("--qmax", type=int, default=24, help="served: largest qubit count")
+    ap.add_argument("--count", type=int, default=0, help="circuits (batched: 512; served: 20000 per rate)")
+    ap.add_argument("--rates", default="50,200,500,1000,2000", help="served: arrival rates per second")
+    ap.add_argument("--qmax", type=int, default=30, help="served: largest qubit count")
     ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"], help="served: admission order")
     ap.add_argument("--compile-on-arrival", action="store_true",
                     help="served: compile each request when it arrives (spawned worker pool) instead of before "

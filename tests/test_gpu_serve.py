@@ -57,8 +57,50 @@ def test_budget_limits_resident_memory(torch):
     srv = Server(budget_bytes=budget, max_inflight=8)
     done = srv.run([Request(i, gen.random_layer(16, 6, i), 0.0) for i in range(10)])
     assert len(done) == 10 and srv.stats["peak_bytes"] <= budget and srv.used == 0
-    with pytest.raises(MemoryError):
-        Server(budget_bytes=Server.footprint(16) - 1).run([Request(0, gen.random_layer(16, 2, 0), 0.0)])
+    # a request whose state can never fit is rejected on its own; the server does not stop
+    small = Server(budget_bytes=Server.footprint(16) - 1)
+    done = small.run([Request(0, gen.random_layer(16, 2, 0), 0.0), Request(1, gen.random_layer(12, 2, 1), 0.0)])
+    assert [r.rid for r in done] == [1]
+    assert [r.rid for r, _ in small.failed] == [0] and "exceeds the HBM budget" in small.failed[0][1]
+
+
+@pytest.mark.timeout(600)
+def test_poisoned_requests_fail_alone(torch):
+    """Faults injected on the host into single requests of a served mix: a program with a corrupted word
+    (one small request, run in a whole-circuit batch, and one large), a circuit that does not compile (an
+    unknown gate) and a request whose state is larger than the budget's largest block. Each of those fails
+    alone with its reason; every other request completes with the same result as when it is served alone."""
+    from qsv_b200.circuit import Circuit
+    from qsv_b200.serve import _compile_request
+    reqs = _requests(24, 3000.0, 11)
+
+    def corrupt(r):
+        Server._finish_compile(r, _compile_request((r.circuit, None, 12)))
+        seg = np.array(r.program[0], dtype=np.int32, copy=True)
+        seg[0] ^= 0x1                       # the QSV2 magic word
+        r.program = [seg] + list(r.program[1:])
+
+    small_bad = next(r for r in reqs if r.circuit.num_qubits <= 13)
+    large_bad = next(r for r in reqs if r.circuit.num_qubits > 13)
+    corrupt(small_bad)
+    corrupt(large_bad)
+    nocompile = next(r for r in reqs[5:] if r not in (small_bad, large_bad))
+    bad = Circuit(nocompile.circuit.num_qubits)
+    bad.append("no_such_gate", [0], [])
+    nocompile.circuit = bad
+    big = Request(1000, gen.random_layer_ccx(23, 3, 5), reqs[10].arrival)
+    srv = Server(budget_bytes=32 << 20, max_inflight=6)         # largest block 32 MiB: at most 22 qubits
+    done = srv.run(reqs + [big])
+    failed = {r.rid: why for r, why in srv.failed}
+    assert set(failed) == {small_bad.rid, large_bad.rid, nocompile.rid, big.rid}, failed
+    assert "engine rejected" in failed[small_bad.rid] and "engine rejected" in failed[large_bad.rid]
+    assert "compile" in failed[nocompile.rid] and "budget" in failed[big.rid]
+    assert len(done) == len(reqs) - 3 and engine.device_status() == 0 and srv.used == 0
+    skip = {small_bad.rid, large_bad.rid, nocompile.rid}
+    alone = {r.rid: r for r in plain_serve([r for r in _requests(24, 1e9, 11) if r.rid not in skip])}
+    for r in done:
+        a = alone[r.rid]
+        assert r.result[0] == a.result[0] and np.array_equal(r.result[1], a.result[1])
 
 
 @pytest.mark.timeout(600)

@@ -45,3 +45,40 @@ def test_ready_queue_orders():
     assert drain(fill(_ReadyQueue("sjf", max_wait=10.0)), 0.5) == [1, 3, 2, 4, 0]
     assert drain(fill(_ReadyQueue("sjf", max_wait=0.2)), 0.35) == [0, 1, 3, 2, 4]
     assert drain(fill(_ReadyQueue("fifo")), 0.5) == [0, 1, 2, 3, 4]
+
+
+def test_state_arena_buddy_allocation():
+    """The server's HBM arena (host tensors here): the budget splits into power-of-two roots; blocks are
+    power-of-two sized and aligned to their size; freed buddies merge back; a block larger than every root
+    never fits."""
+    import torch
+    from qsv_b200.serve import StateArena
+    budget = (1 << 20) + (1 << 18) + 5000          # roots of 1 MiB and 256 KiB; the 5000-byte rest is unused
+    ar = StateArena(budget, torch.device("cpu"))
+    assert ar.capacity == (1 << 20) + (1 << 18) and ar.max_order == 20
+    assert not ar.fits_ever((1 << 20) + 1) and ar.fits_ever(1 << 20)
+    rng = np.random.default_rng(0)
+    live = []
+    for step in range(400):
+        if live and (rng.random() < 0.45 or ar.used > ar.capacity * 0.8):
+            h = live.pop(int(rng.integers(len(live))))
+            ar.release(h)
+            continue
+        size = 1 << int(rng.integers(13, 19))
+        h = ar.alloc(size)
+        if h is None:
+            continue
+        root, off, o = h
+        assert (1 << o) >= size and off % (1 << o) == 0 and off + (1 << o) <= (1 << ar.roots[root][1])
+        for r2, off2, o2 in live:                  # no two live blocks overlap
+            if r2 == root:
+                assert off + (1 << o) <= off2 or off2 + (1 << o2) <= off
+        live.append(h)
+        assert ar.used == sum(1 << x[2] for x in live)
+        v = ar.view(h, o - 3)
+        assert v.dtype == torch.complex64 and v.numel() == (1 << o) // 8
+    for h in live:
+        ar.release(h)
+    assert ar.used == 0
+    # everything merged back: the two whole roots are free again
+    assert ar.alloc(1 << 20) is not None and ar.alloc(1 << 18) is not None and ar.alloc(1 << 13) is None

@@ -9,6 +9,13 @@ whole-circuit batch launch, larger ones each run their sweeps on their own strea
 detected with CUDA events; the result (norm and <Z_q> per qubit, FP64, plus the state if asked) is read
 back and the memory released. Each request's arithmetic is independent of the others (no cross-request
 reduction, fixed op order), so a result is the same alone and in the mix.
+
+The HBM budget is real memory: the server reserves it once as an arena and gives every admitted state a
+power-of-two block of it (buddy allocation; a 2^n-amplitude complex64 state is exactly 2^(n+3) bytes), so
+admission never depends on the caching allocator's fragmentation and the footprint stays fixed while the
+server runs. A request that cannot be served (its state can never fit the arena, its circuit does not
+compile, its program is rejected by the engine) fails alone: it is recorded in ``Server.failed`` with the
+reason and every other request runs on.
 """
 import heapq
 import math
@@ -40,6 +47,82 @@ class Request:
     result: object = None
     state: object = None
     work: int = 0                   # estimated device work: 2^n x op records of the program
+    error: str = None               # why the request could not be served (None: served)
+
+
+class StateArena:
+    """The server's HBM budget, reserved once, handed out as power-of-two blocks (binary buddy system).
+
+    The budget is split into power-of-two root blocks (largest first, each at most 2^37 bytes); a request
+    for 2^order bytes takes the smallest free block of at least that size, splitting it in halves; a freed
+    block merges with its free buddy. Blocks are 2^order bytes at offsets that are multiples of 2^order
+    within their root, so every state is aligned to its own size. Host-side bookkeeping only: reuse is safe
+    because a block is freed only after the work on it has completed (its CUDA event)."""
+
+    MIN_ORDER = 13               # 8 KiB: the smallest state the engine runs (2^10 complex64)
+    MAX_ROOT_ORDER = 37          # 128 GiB
+
+    def __init__(self, budget_bytes, device):
+        import torch
+        self.roots = []          # (tensor, order)
+        self.free = {}           # order -> set of (root index, offset)
+        left = int(budget_bytes)
+        order = self.MAX_ROOT_ORDER
+        while order >= self.MIN_ORDER and left >= (1 << self.MIN_ORDER):
+            if left >= (1 << order):
+                t = torch.empty(1 << order, dtype=torch.uint8, device=device)
+                self.free.setdefault(order, set()).add((len(self.roots), 0))
+                self.roots.append((t, order))
+                left -= 1 << order
+            else:
+                order -= 1
+        self.capacity = sum(1 << o for _, o in self.roots)
+        self.used = 0
+        self.max_order = max((o for _, o in self.roots), default=-1)
+
+    @staticmethod
+    def order_for(nbytes):
+        return max(StateArena.MIN_ORDER, int(nbytes - 1).bit_length())
+
+    def fits_ever(self, nbytes):
+        return self.order_for(nbytes) <= self.max_order
+
+    def alloc(self, nbytes):
+        """-> (root index, offset, order), or None when no free block is large enough right now."""
+        want = self.order_for(nbytes)
+        o = want
+        while o <= self.max_order and not self.free.get(o):
+            o += 1
+        if o > self.max_order:
+            return None
+        blk = min(self.free[o])               # lowest root / offset first: packs work toward the front
+        self.free[o].discard(blk)
+        root, off = blk
+        while o > want:                       # split, keeping the lower half
+            o -= 1
+            self.free.setdefault(o, set()).add((root, off + (1 << o)))
+        self.used += 1 << want
+        return root, off, want
+
+    def release(self, handle):
+        root, off, o = handle
+        self.used -= 1 << o
+        root_order = self.roots[root][1]
+        while o < root_order:
+            buddy = (root, off ^ (1 << o))
+            if buddy not in self.free.get(o, ()):
+                break
+            self.free[o].discard(buddy)
+            off = min(off, buddy[1])
+            o += 1
+        self.free.setdefault(o, set()).add((root, off))
+
+    def view(self, handle, n):
+        """The block as a 2^n-amplitude complex64 state tensor."""
+        import torch
+        root, off, o = handle
+        t = self.roots[root][0]
+        return t[off: off + (8 << n)].view(torch.complex64)
 
 
 @dataclass
@@ -50,7 +133,7 @@ class _Slot:
     event: object
     scratch: object
     zout: object
-    bytes: int
+    handle: tuple
 
 
 def config5_requests(count=20000, rate=50.0, seed=4, qmin=12, qmax=30, dmin=10, dmax=100):
@@ -137,13 +220,16 @@ class Server:
         engine.load()
         self.device = torch.device(device if device is not None else "cuda")
         self.budget = int(budget_bytes)
+        self.arena = StateArena(self.budget, self.device)
+        self.failed = []             # (request, reason) of requests that could not be served
         self.max_inflight = max_inflight
         self.k = k
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max_inflight)]
         self.free_streams = deque(range(max_inflight))
         self.used = 0
         self.policy, self.max_wait = policy, max_wait
-        self.stats = dict(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0)
+        self.stats = dict(admitted=0, small_batches=0, small_in_batches=0, peak_bytes=0, peak_inflight=0,
+                          rejected=0, arena_bytes=self.arena.capacity)
         self.pool = None
         self.compile_workers = compile_workers
         if compile_workers:
@@ -159,15 +245,23 @@ class Server:
             self.pool.map(_warm_one, range(self.compile_workers), chunksize=1)
 
     def close(self):
+        """Stop the compile workers and give the arena back to the device."""
         if self.pool is not None:
             self.pool.terminate()
             self.pool = None
+        self.arena = None
 
     @staticmethod
     def footprint(n):
-        """Device bytes a request holds while in flight: its state, reduction scratch, outputs."""
-        m = max(n, engine.N_MIN)
-        return (8 << m) + engine.scratch_bytes(m) + 8 * (m + 1)
+        """Arena bytes a request's state holds while in flight (its small reduction scratch and outputs come
+        from the caching allocator, at most max_inflight of them)."""
+        return 8 << max(n, engine.N_MIN)
+
+    def _reject(self, req, reason, now):
+        req.error = reason
+        req.done = now
+        self.failed.append((req, reason))
+        self.stats["rejected"] += 1
 
     def _compile(self, req):
         self._finish_compile(req, _compile_request((req.circuit, req.spec, self.k)))
@@ -179,7 +273,9 @@ class Server:
         req.work = (1 << req.n) * sum(len(seg) for seg in req.program)
 
     def _launch(self, reqs, now):
-        """Start a group of admitted requests: small ones as one whole-circuit batch, large ones alone."""
+        """Start a group of admitted requests: small ones as one whole-circuit batch, large ones alone. A
+        request whose program the engine rejects (checked on the host before anything of it is queued)
+        fails alone; the others of its group still run."""
         import torch
         slots = []
         small = [r for r in reqs if r.n <= SMALL_MAX]
@@ -188,31 +284,48 @@ class Server:
         for grp in groups:
             si = self.free_streams.popleft()
             st = self.streams[si]
-            # every buffer of the group is allocated on the group's stream, so the caching allocator
-            # never hands it to other work before this stream is done with it
+            members = []                 # (request, arena block, state) that run
+            batch = None
+            # the small outputs and scratch are allocated on the group's stream, so the caching allocator
+            # never hands them to other work before this stream is done with them
             with torch.cuda.stream(st):
-                states = [engine.new_state(r.n, device=self.device, zero=True, stream=st) for r in grp]
-                batch = None
                 if grp is small:
                     batch = engine.SmallBatch()
-                    for r, s in zip(grp, states):
-                        batch.add(s, r.program)
+                for r in grp:
+                    h = self._handles.pop(r.rid)
+                    s = self.arena.view(h, r.n)
+                    try:
+                        if batch is not None:
+                            batch.add(s, r.program)          # host-side decode and checks
+                        else:
+                            engine.zero_state(s, st)
+                            for seg in r.program:
+                                engine.run_segment(s, seg, st)
+                    except (engine.QSVError, ValueError) as e:
+                        st.synchronize()                     # what was queued for it has drained
+                        self.arena.release(h)
+                        self._reject(r, f"engine rejected the program: {e}", now)
+                        continue
+                    members.append((r, h, s))
+                if not members:
+                    self.free_streams.append(si)
+                    continue
+                if batch is not None:
+                    for _, _, s in members:
+                        engine.zero_state(s, st)
                     batch.upload(st)
                     batch.launch(st)
                     self.stats["small_batches"] += 1
-                    self.stats["small_in_batches"] += len(grp)
-                else:
-                    for seg in grp[0].program:
-                        engine.run_segment(states[0], seg, st)
+                    self.stats["small_in_batches"] += len(members)
                 outs = []
-                for r, s in zip(grp, states):
+                for r, _, s in members:
                     sc = engine.new_scratch(r.n, self.device)
                     outs.append((sc, engine.reduce_f64(s, scratch=sc, stream=st)))
                 ev = torch.cuda.Event()
                 ev.record(st)
-            for r, s, (sc, z) in zip(grp, states, outs):
+            for (r, h, s), (sc, z) in zip(members, outs):
                 r.admitted = now
-                slot = _Slot(r, si, s, ev, sc, z, self.footprint(r.n))
+                slot = _Slot(r, si, s, ev, sc, z, h)
                 slot.batch = batch           # the batch tables stay alive until the group completes
                 slots.append(slot)
         return slots
@@ -225,6 +338,7 @@ class Server:
         ready = _ReadyQueue(self.policy, self.max_wait)
         inflight = []
         done = []
+        self._handles = {}
         t0 = time.perf_counter()
         while pending or compiling or ready.peek(time.perf_counter() - t0) is not None or inflight:
             now = time.perf_counter() - t0
@@ -237,25 +351,32 @@ class Server:
                 if r.program is not None:
                     ready.append(r)
                 elif self.pool is None:
-                    self._compile(r)
-                    ready.append(r)
+                    try:
+                        self._compile(r)
+                        ready.append(r)
+                    except Exception as e:        # this request's circuit does not compile: it fails alone
+                        self._reject(r, f"compile failed: {e}", now)
                 else:
                     compiling.append((r, self.pool.apply_async(_compile_request, ((r.circuit, r.spec, self.k),))))
                 if self.pool is None and realtime:
                     break                 # compile inline one at a time, keep the device fed meanwhile
-            if self.policy == "fifo":
-                while compiling and compiling[0][1].ready():      # arrival order
-                    r, fut = compiling.popleft()
+            def take_compiled(r, fut):
+                try:
                     self._finish_compile(r, fut.get())
                     ready.append(r)
+                except Exception as e:            # the worker's compilation raised: this request fails alone
+                    self._reject(r, f"compile failed: {e}", now)
+
+            if self.policy == "fifo":
+                while compiling and compiling[0][1].ready():      # arrival order
+                    take_compiled(*compiling.popleft())
             elif compiling:
                 # shortest-work-first: every finished compilation joins the ready queue at once (a long
                 # compilation ahead of it does not hold it back)
                 still = deque()
                 for r, fut in compiling:
                     if fut.ready():
-                        self._finish_compile(r, fut.get())
-                        ready.append(r)
+                        take_compiled(r, fut)
                     else:
                         still.append((r, fut))
                 compiling = still
@@ -268,12 +389,17 @@ class Server:
                 if r is None:
                     break
                 fp = self.footprint(r.n)
-                if self.used + fp > self.budget:
-                    if not inflight and not admit:
-                        raise MemoryError(f"request {r.rid} ({r.n} qubits) exceeds the HBM budget")
-                    break
+                if not self.arena.fits_ever(fp):
+                    # its state is larger than any block the budget can ever give: reject it, serve the rest
+                    ready.take(r)
+                    self._reject(r, f"{r.n}-qubit state ({fp} B) exceeds the HBM budget's largest block", now)
+                    continue
+                h = self.arena.alloc(fp)
+                if h is None:
+                    break                 # waits for running requests to free their blocks
                 ready.take(r)
-                self.used += fp
+                self._handles[r.rid] = h
+                self.used = self.arena.used
                 admit.append(r)
                 if r.n <= SMALL_MAX:
                     if not small_group:
@@ -301,7 +427,8 @@ class Server:
                         dst = torch.empty_like(sl.state)
                         engine.remap(sl.state, dst, perm)
                         r.state = dst.cpu().numpy()[: 1 << n_log]
-                    self.used -= sl.bytes
+                    self.arena.release(sl.handle)
+                    self.used = self.arena.used
                     finished_streams.add(sl.stream)
                     done.append(r)
                 else:
@@ -335,12 +462,13 @@ def precompile(requests, workers=0):
     return requests
 
 
-def plain_serve(requests, device=None):
+def plain_serve(requests, device=None, k=12):
     """The plain sequential path: each request alone, in arrival order (a single FIFO server, no overlap;
     requests without a program are compiled when they are served). Returns the completed requests with
-    admitted/done times on the same arrival clock."""
+    admitted/done times on the same arrival clock; a request that cannot run (compile or engine error)
+    gets its `error` set and is left out."""
     import torch
-    srv = Server(max_inflight=1, device=device)
+    dev = torch.device(device if device is not None else "cuda")
     pending = sorted(requests, key=lambda r: r.arrival)
     t0 = time.perf_counter()
     out = []
@@ -348,25 +476,29 @@ def plain_serve(requests, device=None):
         now = time.perf_counter() - t0
         if r.arrival > now:
             time.sleep(r.arrival - now)
-        if r.program is None:
-            srv._compile(r)
-        r.admitted = time.perf_counter() - t0
-        st = engine.new_state(r.n, device=srv.device)
-        if r.n <= SMALL_MAX:
-            b = engine.SmallBatch()
-            b.add(st, r.program)
-            b.upload()
-            b.launch()
-        else:
-            for seg in r.program:
-                engine.run_segment(st, seg)
+        try:
+            if r.program is None:
+                Server._finish_compile(r, _compile_request((r.circuit, r.spec, k)))
+            r.admitted = time.perf_counter() - t0
+            st = engine.new_state(r.n, device=dev)
+            if r.n <= SMALL_MAX:
+                b = engine.SmallBatch()
+                b.add(st, r.program)
+                b.upload()
+                b.launch()
+            else:
+                for seg in r.program:
+                    engine.run_segment(st, seg)
+        except Exception as e:
+            r.error = f"{type(e).__name__}: {e}"
+            continue
         z = engine.reduce_f64(st).cpu().numpy()
         r.done = time.perf_counter() - t0
         n_log = r.n_log
         r.result = (float(z[0]), np.array([z[1 + r.fmap[q]] for q in range(n_log)]))
         out.append(r)
         del st
-    torch.cuda.synchronize(srv.device)
+    torch.cuda.synchronize(dev)
     return out
 
 
