@@ -109,14 +109,14 @@ def statevector_f64(qc, n=None):
     st = np.zeros(1 << n, dtype=np.complex128)
     st[0] = 1
     skip = {"measure", "barrier", "delay", "save_statevector", "id"}
-    mc_names = {"ccx", "ccz", "c3x", "c4x", "mcx", "mcx_gray", "mcx_recursive", "mcp", "mcphase"}
+    mc_names = {"ccx", "ccz", "c3x", "c4x", "mcx", "mcx_gray", "mcx_recursive", "mcp", "mcphase", "c3sx"}
     for name, qs, params in pkg.circuit.normalize(qc):
         if name in skip:
             continue
         if name in mc_names:
             apply_controlled(st, qs[:-1], qs[-1], pkg.gates.mc_matrix(name, len(qs) - 1, params))
         else:
-            apply_dense(st, qs, pkg.gates.gate_matrix(name, params))
+            apply_dense(st, qs, pkg.gates.gate_matrix(name, params, len(qs)))
     return st
 
 

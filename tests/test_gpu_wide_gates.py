@@ -1,0 +1,59 @@
+"""Wide multi-controlled gates and the newly supported gates on the GPU, through SVRuntime.run: Grover at 14
+and 16 qubits with the default window (k = 12; its mcx covers every qubit, so the compiler lowers it with the
+Barenco et al. constructions), an mcx over 16 qubits after a random product state, and rccx / rcccx / c3sx /
+ms. Each result against the dense FP64 oracle: 1 - F <= 1e-5 (tests/functional_suite.py:92-94)."""
+import numpy as np
+import pytest
+
+from qsv_b200 import engine, generators as gen
+from qsv_b200.circuit import Circuit
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rt():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    from qsv_b200.runtime import SVRuntime
+    return SVRuntime()
+
+
+def _check(rt, qc):
+    r = rt.run(qc, shots=0, return_state=True)
+    m = orc.metrics(orc.statevector_f64(qc), r["state"])
+    assert engine.device_status() == 0
+    assert m["one_minus_f"] <= 1e-5 and abs(m["norm"] - 1) <= 1e-4, m
+    return r
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("n", [14, 16])
+def test_grover_beyond_window(rt, n):
+    r = _check(rt, gen.grover(n))
+    assert r["stats"]["lowered"].get("mcx", 0) > 0
+
+
+@pytest.mark.timeout(600)
+def test_mcx16_after_product_state(rt):
+    rng = np.random.default_rng(16)
+    qc = Circuit(16)
+    for i in range(16):
+        qc.u(*[float(v) for v in rng.uniform(0, 2 * np.pi, 3)], i)
+    qs = [int(x) for x in rng.permutation(16)]
+    qc.mcx(qs[:-1], qs[-1])
+    for i in range(16):
+        qc.rx(0.3 + 0.05 * i, i)
+    _check(rt, qc)
+
+
+@pytest.mark.parametrize("name,nq,params", [("rccx", 3, ()), ("rcccx", 4, ()), ("c3sx", 4, ()), ("ms", 5, (0.6,))])
+def test_defined_gates(rt, name, nq, params):
+    rng = np.random.default_rng(nq)
+    qc = Circuit(12)
+    for i in range(12):
+        qc.u(*[float(v) for v in rng.uniform(0, 2 * np.pi, 3)], i)
+    qc.append(name, [int(x) for x in rng.permutation(12)[:nq]], params)
+    _check(rt, qc)

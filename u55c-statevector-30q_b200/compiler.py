@@ -7,6 +7,9 @@ reference yields the same QSV2 words (the golden-stream tests check this word fo
 Qiskit: gate matrices come from ``gates.py`` and wide gates are lowered by ``_lower`` below instead of
 ``qiskit.transpile``.
 
+Multi-controlled gates wider than the tile window become several narrower controlled gates (``_mc_plan``,
+the constructions of Barenco et al. 1995), where the reference transpiles them to CX and one-qubit gates.
+
 Program = list of steps, executed in order by the runtime:
   ("segment", int32 words)  one engine launch (every pass of the segment over the whole state)
   ("remap", perm)           qubit permutation, perm[new_phys] = old_phys
@@ -14,15 +17,16 @@ Program = list of steps, executed in order by the runtime:
 from dataclasses import dataclass, field
 
 import numpy as np
-from scipy.linalg import cossin
+from scipy.linalg import cossin, schur
 
 from .isa import MAGIC, OP_MUX2, MAX_OPS_PER_PASS, MAX_HIGH, DTYPE_C64, DTYPE_C128
-from .gates import I2, X, Z, gate_matrix, mc_matrix, phase
+from .gates import DEFINITIONS, I2, X, Z, definition, gate_matrix, mc_matrix, phase
 from .circuit import normalize
 
 SKIP = {"measure", "barrier", "delay", "save_statevector", "id"}   # compiler.py:20
 # multi-controlled gates built directly as one MUX2 (controls all-ones select U), compiler.py:25-29
-MC_NAMES = {"ccx", "c3x", "c4x", "mcx", "mcx_gray", "mcx_recursive", "ccz", "mcphase", "mcp"}
+# ("_mcu" is the compiler's own: a controlled 2x2 matrix produced by _mc_plan, carried as its parameter)
+MC_NAMES = {"ccx", "c3x", "c4x", "mcx", "mcx_gray", "mcx_recursive", "ccz", "mcphase", "mcp", "c3sx", "_mcu"}
 MAX_DENSE_QUBITS = 10     # wider gates are never expanded to a dense matrix (compiler.py:132)
 
 
@@ -131,8 +135,57 @@ def _lower(name, nq, params):
     gate sequence differs from Qiskit's but implements the same unitary. Qubits are gate-local."""
     if name == "cswap":
         return [("cx", (2, 1), ()), ("ccx", (0, 1, 2), ()), ("cx", (2, 1), ())]
+    if name in DEFINITIONS:             # rccx, rcccx: their basis-gate definitions
+        return definition(name)
+    if name == "ms":                    # global Molmer-Sorensen: rxx(theta) on every pair (they commute)
+        return [("rxx", (i, j), (params[0],)) for i in range(nq) for j in range(i + 1, nq)]
     raise NotImplementedError(
         f"gate {name!r} on {nq} qubits is neither a (multi-)controlled 2x2 nor wide-gate lowerable here")
+
+
+def _sqrt2(U):
+    """Principal square root of a 2x2 unitary (complex Schur form: U = Z diag(l) Z^dag, unitary Z)."""
+    T, Zm = schur(np.asarray(U, dtype=complex), output="complex")
+    return Zm @ np.diag(np.sqrt(np.diag(T))) @ Zm.conj().T
+
+
+def _is_x(U):
+    return np.array_equal(np.asarray(U), X)
+
+
+def _mc_plan(ctrls, t, U, width, spare):
+    """A multi-controlled 2x2 gate (U on qubit t when every qubit of `ctrls` is 1) as a sequence of
+    controlled 2x2 gates of at most `width` qubits each: [(controls, target, 2x2 matrix)], in time order.
+    `spare`: qubits outside the gate; they may be borrowed in any state and are returned unchanged.
+
+    Constructions of Barenco et al., "Elementary gates for quantum computation", Phys. Rev. A 52, 3457
+    (1995):
+      * with a borrowed qubit g and the controls split into A and B (Lemma 7.2's one-ancilla form):
+            C_{A+B}(X)_t = C_A(X)_g . C_{B+g}(X)_t . C_A(X)_g . C_{B+g}(X)_t     (time order)
+        -- the first and third flip g by AND(A), so the two C_{B+g}(X) together flip t by AND(A)AND(B)
+        whatever g held, and g ends as it started;
+      * with no qubit to borrow, or a target matrix other than X (Lemma 7.5), V^2 = U, q one control, R the
+        others:
+            C_{R+q}(U)_t = C_q(V)_t . C_R(X)_q . C_q(V^dag)_t . C_R(X)_q . C_R(V)_t   (time order)
+        -- the two C_R(X)_q may borrow t; C_R(V)_t has one control fewer and q becomes free.
+    Both are exact identities, so the plan implements U exactly (up to the rounding of V to FP32 when
+    the ops are encoded)."""
+    ctrls = list(ctrls)
+    if len(ctrls) + 1 <= width:
+        return [(tuple(ctrls), t, U)]
+    if _is_x(U) and spare:
+        g = spare[0]
+        rest = spare[1:]
+        a = max(1, min(width - 1, len(ctrls) - 1))       # A fills a native gate; B keeps the rest
+        A, B = ctrls[:a], ctrls[a:]
+        on_g = _mc_plan(A, g, X, width, [t] + B + rest)
+        on_t = _mc_plan(B + [g], t, X, width, A + rest)
+        return on_g + on_t + on_g + on_t
+    q, R = ctrls[-1], ctrls[:-1]
+    V = _sqrt2(U)
+    flip = _mc_plan(R, q, X, width, [t] + list(spare))
+    return ([((q,), t, V)] + flip + [((q,), t, V.conj().T)] + flip +
+            _mc_plan(R, t, V, width, [q] + list(spare)))
 
 
 def circuit_to_ops(qc, stats, fuse_1q=True, max_width=None):
@@ -179,7 +232,7 @@ def circuit_to_ops(qc, stats, fuse_1q=True, max_width=None):
                 _count(stats.native, name)
             lower(name, qs, params)
             return
-        M = gate_matrix(name, params)
+        M = gate_matrix(name, params, nq)
         if not lowered:
             _count(stats.native, name)
         if nq == 1:
@@ -205,6 +258,16 @@ def circuit_to_ops(qc, stats, fuse_1q=True, max_width=None):
     def lower(name, qs, params):
         _count(stats.native, name, -1)
         _count(stats.lowered, name)
+        if name in MC_NAMES:
+            # wider than the window: narrower controlled gates (the circuit's other qubits may be borrowed)
+            width = max_width if max_width is not None else MAX_DENSE_QUBITS
+            inside = set(qs)
+            spare = [x for x in range(n) if x not in inside]
+            U = mc_matrix(name, len(qs) - 1, params)
+            for ctrls, t, M in _mc_plan(list(qs[:-1]), qs[-1], U, width, spare):
+                sub = "_u1m" if not ctrls else "_cum" if len(ctrls) == 1 else "_mcu"
+                handle(sub, list(ctrls) + [t], (M,), True)
+            return
         for sub_name, sub_qs, sub_params in _lower(name, len(qs), params):
             handle(sub_name, [qs[i] for i in sub_qs], sub_params, True)
 

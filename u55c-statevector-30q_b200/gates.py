@@ -125,7 +125,9 @@ _FIXED = {
     "csdg": _const(controlled(SDG)), "swap": _const(SWAP), "iswap": _const(ISWAP), "ecr": _const(ECR),
     "dcx": _const(DCX), "ccx": _const(controlled(X, 2)), "ccz": _const(controlled(Z, 2)),
     "cswap": _const(cswap()), "c3x": _const(controlled(X, 3)), "c4x": _const(controlled(X, 4)),
+    "c3sx": _const(controlled(SX, 3)),
 }
+_DEFINED = {}
 _XX, _YY, _ZZ, _ZX = _kron_le(X, X), _kron_le(Y, Y), _kron_le(Z, Z), _kron_le(Z, X)
 # parameterised multi-qubit gates: name -> builder(params)
 _PARAM = {
@@ -140,8 +142,80 @@ _PARAM = {
 }
 
 
-def gate_matrix(name, params=()):
-    """Dense Qiskit-convention matrix of a named gate (1q, 2q and the supported multi-qubit gates)."""
+# Gates defined by a short sequence of basis gates (OpenQASM 2's qelib1.inc definitions): the relative-
+# phase Toffolis. Gate-local qubits; the dense matrix is the product of the sequence, and the compiler lowers
+# the gate to the sequence itself (neither is a controlled 2x2).
+_U2_0PI = ("u2", (0.0, math.pi))
+_T_ = ("u1", (math.pi / 4,))
+_TDG_ = ("u1", (-math.pi / 4,))
+DEFINITIONS = {
+    # rccx a, b, c: simplified (Margolus) Toffoli, equal to ccx up to relative phases
+    "rccx": (3, [(_U2_0PI, (2,)), (_T_, (2,)), (("cx", ()), (1, 2)), (_TDG_, (2,)), (("cx", ()), (0, 2)),
+                 (_T_, (2,)), (("cx", ()), (1, 2)), (_TDG_, (2,)), (_U2_0PI, (2,))]),
+    # rcccx (rc3x) a, b, c, d: relative-phase 3-controlled X
+    "rcccx": (4, [(_U2_0PI, (3,)), (_T_, (3,)), (("cx", ()), (2, 3)), (_TDG_, (3,)), (_U2_0PI, (3,)),
+                  (("cx", ()), (0, 3)), (_T_, (3,)), (("cx", ()), (1, 3)), (_TDG_, (3,)), (("cx", ()), (0, 3)),
+                  (_T_, (3,)), (("cx", ()), (1, 3)), (_TDG_, (3,)), (_U2_0PI, (3,)), (_T_, (3,)),
+                  (("cx", ()), (2, 3)), (_TDG_, (3,)), (_U2_0PI, (3,))]),
+}
+
+
+def definition(name):
+    """[(gate name, gate-local qubits, params), ...] of a gate in DEFINITIONS."""
+    return [(g, qs, p) for (g, p), qs in DEFINITIONS[name][1]]
+
+
+def _embed(M, qubits, nq):
+    """Dense 2^nq matrix of gate M acting on the given gate-local qubits (little-endian order)."""
+    d = 1 << nq
+    k = len(qubits)
+    out = np.zeros((d, d), dtype=complex)
+    for col in range(d):
+        sub = sum(((col >> q) & 1) << i for i, q in enumerate(qubits))
+        rest = col & ~sum(1 << q for q in qubits)
+        for row_sub in range(1 << k):
+            v = M[row_sub, sub]
+            if v != 0:
+                row = rest | sum(((row_sub >> i) & 1) << q for i, q in enumerate(qubits))
+                out[row, col] += v
+    return out
+
+
+def _defined_matrix(name):
+    nq = DEFINITIONS[name][0]
+    M = np.eye(1 << nq, dtype=complex)
+    for g, qs, p in definition(name):
+        M = _embed(gate_matrix(g, p), qs, nq) @ M
+    return _const(M)
+
+
+def ms_matrix(nq, theta):
+    """Global Molmer-Sorensen gate on nq qubits: the product of rxx(theta) over every qubit pair (the pair
+    terms commute)."""
+    M = np.eye(1 << nq, dtype=complex)
+    R = _expm_herm(_XX, theta)
+    for i in range(nq):
+        for j in range(i + 1, nq):
+            M = _embed(R, (i, j), nq) @ M
+    return M
+
+
+def gate_matrix(name, params=(), nq=None):
+    """Dense Qiskit-convention matrix of a named gate (1q, 2q and the supported multi-qubit gates). nq is
+    needed only by gates of variable width (ms)."""
+    if name == "_u1m":                  # compiler-internal: a 2x2 matrix carried as the parameter
+        return params[0]
+    if name == "_cum":                  # compiler-internal: the 2x2 parameter controlled by gate qubit 0
+        return controlled(params[0])
+    if name in DEFINITIONS:
+        M = _DEFINED.get(name)
+        if M is None:
+            M = _DEFINED[name] = _defined_matrix(name)
+        return M
+    if name == "ms":
+        if nq is None:
+            raise KeyError("ms needs its number of qubits")
+        return ms_matrix(nq, float(params[0]))
     if name in _ONE:
         npar, f = _ONE[name]
         return f(*[float(x) for x in params[:npar]]) if npar else f()
@@ -160,6 +234,10 @@ def mc_matrix(name, n_ctrl, params=()):
         return X
     if name == "ccz":
         return Z
+    if name == "c3sx":
+        return SX
     if name in ("mcp", "mcphase"):
         return phase(float(params[0]))
+    if name == "_mcu":                  # compiler-internal: the 2x2 target matrix carried as the parameter
+        return params[0]
     raise KeyError(name)

@@ -31,9 +31,11 @@ _NATIVE = {
     "cp": (1, 2), "cu1": (1, 2), "crx": (1, 2), "cry": (1, 2), "crz": (1, 2), "cu3": (3, 2), "cu": (4, 2),
     "rxx": (1, 2), "ryy": (1, 2), "rzz": (1, 2), "rzx": (1, 2),
     "ccx": (0, 3), "ccz": (0, 3), "cswap": (0, 3), "c3x": (0, 4), "c4x": (0, 5),
+    "rccx": (0, 3), "rc3x": (0, 4), "c3sqrtx": (0, 4),
 }
-_RENAME = {"u3": "u", "U": "u", "u1": "p", "CX": "cx"}
-_EXPORT = {"u": "u3"}
+# qelib1 names -> this package's (Qiskit's) names, and back for export
+_RENAME = {"u3": "u", "U": "u", "u1": "p", "CX": "cx", "rc3x": "rcccx", "c3sqrtx": "c3sx"}
+_EXPORT = {"u": "u3", "rcccx": "rc3x", "c3sx": "c3sqrtx"}
 
 _BINOPS = {ast.Add: operator.add, ast.Sub: operator.sub, ast.Mult: operator.mul, ast.Div: operator.truediv,
            ast.Pow: operator.pow}
