@@ -169,36 +169,34 @@ QSV_API int qsv_set_layout13(int rb);
  * shuffles) instead of starting a new phase, 0..2 (default 1). Values are identical either way. */
 QSV_API int qsv_set_phase_lanes(int k);
 
-/* Tuning knob (no reference counterpart): form of the interpreter sweep kernel. 1 (default) = ping-pong:
- * ops whose code path writes every amplitude a thread holds go from one register set to the other, so the
- * run-time dispatch of each op leaves no register reconciliation behind, with tiles staged by the consumer
- * warps themselves (no producer warp, so a thread may hold both register sets); 0 = every op in place,
- * staged by a producer warp; 2 = every op in place, staged by the consumers. Values are identical in every
- * form. Returns the previous form, or QSV_ERR_INVALID_ARG. Process-wide. */
-QSV_API int qsv_set_interp_form(int form);
-
 /* Specialised sweep kernels (no reference counterpart; the reference's engine is one fixed HLS kernel).
  * qsv_run_segment can launch, instead of the interpreter kernel, a kernel compiled at run time (NVRTC,
  * sm_100a) for the sweep's structure: its phase layouts and, per op, target slot, code variant and control
  * masks (everything but the matrices and the window). Values are identical either way.
+ * A coarse structure keeps the layouts and, per op, slot, control masks, kind and whether the matrix is a
+ * swap; its kernel runs every other op with the dense arithmetic (same values) and serves every sweep of
+ * that coarse structure, so sweeps whose exact structure never repeats (random gate choices) still share it.
  * mode 0 = interpreter only; 1 = eager: a new structure is compiled (blocking) before its first launch;
  * 2 = automatic (default): a structure is compiled in background threads once its launches have swept
  * 2^31 amplitudes in total (two sweeps of a 30-qubit state, 512 of a 22-qubit one; at most 64 compilations
- * wait at a time), and used from the first launch after its kernel is ready. Switching to mode 0 drops
- * waiting compilations and waits for running ones. Returns the previous mode. Process-wide. */
+ * wait at a time), and used from the first launch after its kernel is ready; until then the sweep runs its
+ * coarse structure's kernel, compiled by the same rule over the work of all sweeps sharing it, or the
+ * interpreter; 3 = eager with coarse structures only. Switching to mode 0 drops waiting compilations and
+ * waits for running ones. Returns the previous mode. Process-wide. */
 QSV_API int qsv_set_jit(int mode);
 
 /* Compile, in parallel and blocking, the specialised kernels of every sweep of a segment for an n-qubit
- * state (host work only; no device is touched). Returns how many of the segment's structures have a
- * ready kernel, or a negative error code for a malformed segment. */
+ * state (host work only; no device is touched): exact structures, or coarse ones in mode 3. Returns how
+ * many of the segment's sweeps have a ready kernel, or a negative error code for a malformed segment. */
 QSV_API int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n);
 
 /* Block until every queued background compilation has finished. */
 QSV_API int qsv_jit_wait(void);
 
-/* Counters of the specialised-kernel cache, written to out[0 .. min(cap, 8)): mode, structures seen,
- * kernels ready, compilations failed, sweeps launched specialised, sweeps launched interpreted, total
- * compile milliseconds, compilations queued or running. Returns 8. */
+/* Counters of the specialised-kernel cache, written to out[0 .. min(cap, 10)): mode, structures seen
+ * (exact and coarse), kernels ready, compilations failed, sweeps launched specialised (exact or coarse),
+ * sweeps launched interpreted, total compile milliseconds, compilations queued or running, sweeps launched
+ * with a coarse structure's kernel, coarse structures seen. Returns 10. */
 QSV_API int qsv_jit_info(long long *out, int cap);
 
 #ifdef __cplusplus

@@ -6,9 +6,9 @@ the load of its first tile (a flag that nothing sets, from the consumers' point 
 limit (qsv_set_wait_limit_us, 20 ms here instead of the default 2 s) the waiting threads give up, set bit 0
 of the status word, the issuing thread waits (bounded) for its other loads still in flight, and the kernel
 ends. The test reads the status, then runs the same segment clean and checks it against the C oracle value
-for value. Covered: the interpreter staged by a producer warp (form 0) and by its consumer warps (form 1),
-a kernel specialised to the sweep's structure, the complex128 kernel, and SVRuntime.run, which raises on a
-set status word. No test here traps, faults or hangs a GPU.
+for value. Covered: the interpreter, a kernel specialised to the sweep's exact structure, a coarse
+structure's kernel, the complex128 kernel, and SVRuntime.run, which raises on a set status word. No test
+here traps, faults or hangs a GPU.
 """
 import numpy as np
 import pytest
@@ -56,19 +56,17 @@ def _run_armed_then_clean(torch, seg, x):
     return bad, engine.device_status(), t.cpu().numpy()
 
 
-@pytest.mark.parametrize("mode", ["interp_producer", "interp_consumers", "specialised"])
+@pytest.mark.parametrize("mode", ["off", "eager", "coarse"])
 def test_bounded_wait_reports_and_gpu_stays_usable(torch, mode):
     n = 20
     prog, _, _ = q.compile_circuit(gen.random_layer(n, 4, 7), n, 12)
     seg = prog[0][1]
     x = _rand_state(n, 9)
     ref = orc.run_segment(x.copy(), seg)
-    old_jit = engine.set_jit("eager" if mode == "specialised" else "off")
-    old_form = engine.set_interp_form(0 if mode == "interp_producer" else 1)
+    old_jit = engine.set_jit(mode)
     try:
         bad, clean, y = _run_armed_then_clean(torch, seg, x)
     finally:
-        engine.set_interp_form(old_form)
         engine.set_jit(old_jit)
     assert bad & 1, f"status word {bad:#x}: the injected skipped load was not reported"
     assert clean == 0

@@ -33,7 +33,6 @@ cudaError_t batch_upload(Batch *b, void *ws, cudaStream_t stream);
 cudaError_t batch_launch(Batch *b, void *ws, int nsm, cudaStream_t stream, int *launches);
 cudaError_t launch_reduce_noalloc(const void *state, int n, int dtype, double *out, cudaStream_t stream, size_t *need);
 size_t noalloc_reduce_capacity();
-int set_interp_form(int form);
 int jit_set_mode(int mode);
 int jit_prepare(const std::vector<QsvSweep> &sweeps);
 void jit_wait();
@@ -117,12 +116,6 @@ int qsv_inject_skip_load(int count) {
     return QSV_OK;
 }
 
-int qsv_set_interp_form(int form) {
-    const int old = qsv::set_interp_form(form);
-    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "interpreter form must be 0, 1 or 2");
-    return old;
-}
-
 int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap) {
     if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
     std::vector<qsv::PhysPass> passes;
@@ -182,7 +175,7 @@ int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int d
 
 int qsv_set_jit(int mode) {
     const int old = qsv::jit_set_mode(mode);
-    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "jit mode must be 0, 1 or 2");
+    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "jit mode must be 0, 1, 2 or 3");
     return old;
 }
 

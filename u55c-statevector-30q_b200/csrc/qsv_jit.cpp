@@ -10,11 +10,22 @@
 // headers, embedded at build time) and loaded into every device that runs it. Matrices, window and tile
 // addressing stay kernel parameters. Specialised and interpreted sweeps compute the same values.
 //
+// Coarse structures: many sweeps differ only in which ops happen to be diagonal, dense or identity (a
+// random circuit picks its one-qubit gates per qubit and layer), so their exact structures never repeat.
+// A sweep's coarse structure keeps its layouts, and per op the slot, the control masks, the kind (uniform /
+// controlled / general) and whether the matrix is a swap, and drops everything that depends on the matrix
+// values: every other op runs the dense fused-multiply-add chain, which gives the same values on diagonal
+// and identity matrices (the skipped terms are exact zeros). A coarse kernel serves every sweep with that
+// coarse structure (a 30-qubit random circuit of depth 10 has 35 sweeps of 35 exact structures but 7
+// coarse ones, the same 7 for other seeds), at the cost of dense arithmetic for the diagonal ops.
+//
 // Modes: 0 = interpreter only; 1 = eager (a new structure is compiled before its first launch);
 // 2 = automatic (default): a structure is compiled in the background once the amplitudes its launches
 // have swept add up to kWorkThreshold (a compilation costs about a second of one host core, worth it
-// for sweeps that run often or over large states), with at most kMaxQueued compilations waiting;
-// launches use the interpreter until the kernel is ready.
+// for sweeps that run often or over large states), with at most kMaxQueued compilations waiting; until
+// then a sweep runs the kernel of its coarse structure, compiled by the same rule with the work of every
+// sweep that shares it (kCoarseThreshold), or the interpreter; 3 = eager, coarse structures only (tests
+// and measurements of the coarse kernels).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -46,6 +57,7 @@ cudaError_t status_word_ptr(int **out);
 namespace {
 
 constexpr double kWorkThreshold = 2147483648.0;   // 2^31 amplitudes: 2 sweeps at 30 qubits, 512 at 22
+constexpr double kCoarseThreshold = 2147483648.0; // the same amount, summed over the sweeps of a coarse key
 constexpr size_t kMaxQueued = 64;
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
@@ -132,6 +144,7 @@ struct Entry {
     std::vector<char> cubin;
     std::string log;
     long long uses = 0;
+    bool coarse = false;        // a coarse structure's kernel (coarse_of)
     double work = 0.0;          // amplitudes swept by this structure's launches
     CUfunction fn[kMaxDevices] = {nullptr};
     int per_sm[kMaxDevices] = {0};
@@ -145,7 +158,7 @@ struct Jit {
     int threads = 0, busy = 0;
     bool stopping = false;      // set at process exit: workers take no new work
     int mode = 2;
-    long long jit_launches = 0, interp_launches = 0, compiled = 0, failed = 0;
+    long long jit_launches = 0, interp_launches = 0, coarse_launches = 0, compiled = 0, failed = 0;
     double compile_ms = 0.0;
     std::string last_log;
 };
@@ -154,6 +167,38 @@ struct Jit {
 Jit &J() {
     static Jit *j = new Jit;
     return *j;
+}
+
+bool is_swap_variant(int v) {
+    return v == QSV_V_UNI_SWAP || v == QSV_V_CTRL_SWAP || v == QSV_V_CTRL_SWAP_SEL;
+}
+
+// The coarse structure of sw: a copy whose ops keep slot, controls, kind and the swap / non-swap split,
+// with every value-dependent field replaced by its dense form (generated code reads only these fields).
+QsvSweep coarse_of(const QsvSweep &sw) {
+    QsvSweep c = sw;
+    for (int o = 0; o < c.nops; o++) {
+        QsvOp &op = c.ops[o];
+        const bool swap = is_swap_variant(op.variant) ||
+                          (op.variant == QSV_V_MUX && op.kind == QSV_K_CTRL && op.cls1 == QSV_M_XSWAP);
+        const bool sel = op.variant == QSV_V_CTRL_DENSE_SEL || op.variant == QSV_V_CTRL_DIAG1_SEL ||
+                         op.variant == QSV_V_CTRL_SWAP_SEL;
+        op.r00 = 0;
+        if (op.kind == QSV_K_UNI) {
+            op.cls = op.cls0 = op.cls1 = swap ? QSV_M_XSWAP : QSV_M_DENSE;
+            op.variant = swap ? QSV_V_UNI_SWAP : QSV_V_UNI_DENSE;
+        } else if (op.kind == QSV_K_CTRL) {
+            op.cls0 = QSV_M_IDENT;
+            op.cls = op.cls1 = swap ? QSV_M_XSWAP : QSV_M_DENSE;
+            if (op.variant != QSV_V_MUX)       // the tile-bit-0-control form stays MUX (its own code path)
+                op.variant = swap ? (sel ? QSV_V_CTRL_SWAP_SEL : QSV_V_CTRL_SWAP)
+                                  : (sel ? QSV_V_CTRL_DENSE_SEL : QSV_V_CTRL_DENSE);
+        } else {
+            op.cls = op.cls0 = op.cls1 = QSV_M_DENSE;
+            op.variant = QSV_V_MUX;
+        }
+    }
+    return c;
 }
 
 std::string key_of(const QsvSweep &sw, int rb, int wb) {
@@ -377,8 +422,8 @@ void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
     j.work.notify_one();
 }
 
-std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
-    const std::string key = key_of(sw, rb, wb);
+std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, bool coarse = false) {
+    const std::string key = (coarse ? "C" : "E") + key_of(sw, rb, wb);
     auto it = j.map.find(key);
     if (it != j.map.end()) return it->second;
     auto e = std::make_shared<Entry>();
@@ -386,6 +431,7 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
     e->rb = rb;
     e->wb = wb;
     e->groups = groups_for(sw, wb);
+    e->coarse = coarse;
     j.map.emplace(key, e);
     return e;
 }
@@ -393,7 +439,7 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb) {
 }  // namespace
 
 int jit_set_mode(int mode) {
-    if (mode < 0 || mode > 2) return -1;
+    if (mode < 0 || mode > 3) return -1;
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
     const int old = j.mode;
@@ -411,6 +457,13 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
     for (const QsvSweep &sw : sweeps) {
         int rb = 0, wb = 0;
         if (layout_for_kw(sw.kw, &rb, &wb)) continue;
+        if (j.mode == 3) {
+            const QsvSweep c = coarse_of(sw);
+            auto e = find_or_add(j, c, rb, wb, true);
+            enqueue(j, e, c);
+            mine.push_back(e);
+            continue;
+        }
         auto e = find_or_add(j, sw, rb, wb);
         enqueue(j, e, sw);
         mine.push_back(e);
@@ -431,17 +484,22 @@ void jit_wait() {
     j.done.wait(lk, [&] { return (j.queue.empty() && j.busy == 0) || j.stopping; });
 }
 
-// stats: mode, structures, ready, failed, launches specialised, launches interpreted, compile ms, queued
+// stats: mode, structures, ready, failed, launches specialised (exact or coarse), launches interpreted,
+// compile ms, queued, launches of coarse kernels, coarse structures
 int jit_info(long long *out, int cap) {
     Jit &j = J();
     std::lock_guard<std::mutex> lk(j.mu);
-    long long ready = 0;
-    for (auto &kv : j.map) ready += kv.second->state == kReady;
-    const long long v[8] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
-                            (long long)j.compile_ms, (long long)(j.queue.size() + j.busy)};
-    const int n = std::min(cap, 8);
+    long long ready = 0, coarse = 0;
+    for (auto &kv : j.map) {
+        ready += kv.second->state == kReady;
+        coarse += kv.second->coarse;
+    }
+    const long long v[10] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
+                             (long long)j.compile_ms, (long long)(j.queue.size() + j.busy), j.coarse_launches,
+                             coarse};
+    const int n = std::min(cap, 10);
     for (int i = 0; i < n; i++) out[i] = v[i];
-    return 8;
+    return 10;
 }
 
 std::string jit_last_log() {
@@ -461,14 +519,29 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     {
         std::unique_lock<std::mutex> lk(j.mu);
         if (j.mode == 0 || !d.ok) { j.interp_launches++; return 0; }
-        e = find_or_add(j, sw, rb, wb);
-        e->uses++;
-        e->work += (double)sw.ntiles * (double)(1 << sw.kw);
-        if (e->state == kNew &&
-            (j.mode == 1 || (e->work >= kWorkThreshold && j.queue.size() < kMaxQueued)))
-            enqueue(j, e, sw);
-        if (j.mode == 1) j.done.wait(lk, [&] { return e->state != kQueued; });
-        if (e->state != kReady) { j.interp_launches++; return 0; }
+        const double work = (double)sw.ntiles * (double)(1 << sw.kw);
+        if (j.mode != 3) {
+            e = find_or_add(j, sw, rb, wb);
+            e->uses++;
+            e->work += work;
+            if (e->state == kNew &&
+                (j.mode == 1 || (e->work >= kWorkThreshold && j.queue.size() < kMaxQueued)))
+                enqueue(j, e, sw);
+            if (j.mode == 1) j.done.wait(lk, [&] { return e->state != kQueued; });
+        }
+        if ((!e || e->state != kReady) && (j.mode == 2 || j.mode == 3)) {
+            // the kernel of the sweep's coarse structure, shared with every sweep of that structure
+            const QsvSweep c = coarse_of(sw);
+            std::shared_ptr<Entry> ce = find_or_add(j, c, rb, wb, true);
+            ce->uses++;
+            ce->work += work;
+            if (ce->state == kNew &&
+                (j.mode == 3 || (ce->work >= kCoarseThreshold && j.queue.size() < kMaxQueued)))
+                enqueue(j, ce, c);
+            if (j.mode == 3) j.done.wait(lk, [&] { return ce->state != kQueued; });
+            if (ce->state == kReady) e = ce;
+        }
+        if (!e || e->state != kReady) { j.interp_launches++; return 0; }
     }
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
@@ -517,6 +590,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     }
     std::lock_guard<std::mutex> lk(j.mu);
     j.jit_launches++;
+    if (e->coarse) j.coarse_launches++;
     return 1;
 }
 

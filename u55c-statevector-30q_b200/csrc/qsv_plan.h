@@ -99,8 +99,7 @@ struct QsvOp {
     uint8_t tbit;               // target tile bit
     uint8_t variant;            // QSV_V_*
     uint8_t r00;                // 1: M0 is dense with m00 real (QSV_M_DENSE_R0 path)
-    uint8_t oop;                // 1: the op's code path writes every slot (qsv_op_writes_every_slot)
-    uint8_t pad[1];
+    uint8_t pad[2];
 };
 
 // complex128 op: the same fields with FP64 matrices. In the complex128 layout tile bits 0-2 are lane bits
@@ -119,8 +118,7 @@ struct QsvOpD {
     uint8_t tbit;
     uint8_t variant;
     uint8_t r00;
-    uint8_t oop;
-    uint8_t pad[5];
+    uint8_t pad[6];
 };
 
 // a (c, c) coefficient pair; plain struct so that host code and NVRTC need no CUDA vector types
@@ -140,25 +138,6 @@ struct alignas(8) float2s {
 #define QSV_SPLAT_M6 9
 #define QSV_SPLAT_M7 10
 #define QSV_SPLAT_NM7 11
-
-#if defined(__CUDACC__)
-#define QSV_HOST_DEVICE __host__ __device__
-#else
-#define QSV_HOST_DEVICE
-#endif
-
-// Whether an op's code path (complex64 layout) writes every slot a thread holds: the interpreter applies
-// such ops out of place, from one register set into the other (qsv_ops_pp.cuh). Tile-bit-0 targets:
-// uniform dense and diagonal matrices. Register and lane targets: uniform dense / diagonal / swap and the
-// general MUX (every pair computed with per-pair coefficients; on a lane bit unless it is a controlled op
-// with a tile-bit-0 control), and on a register bit the branch-free controlled dense form.
-static inline QSV_HOST_DEVICE bool qsv_op_writes_every_slot(int slot, int variant, int kind, int cls0, int cm_c) {
-    if (variant == QSV_V_SKIP) return false;
-    if (slot == QSV_SLOT_COMP) return kind == QSV_K_UNI && (cls0 == QSV_M_DENSE || cls0 == QSV_M_DIAG);
-    const bool uni = variant == QSV_V_UNI_DENSE || variant == QSV_V_UNI_DIAG || variant == QSV_V_UNI_SWAP;
-    if (slot >= QSV_SLOT_LANE0) return uni || (variant == QSV_V_MUX && !(kind == QSV_K_CTRL && cm_c));
-    return uni || variant == QSV_V_MUX || variant == QSV_V_CTRL_DENSE_SEL;
-}
 
 // A phase's thread layout: lane bits 0-2 sit on tile bits lane_lo[0..2] (1, 2, 3 for complex64 unless the
 // sweep is swizzled, see QsvSweepT::swz; 0, 1, 2 for complex128), lane bits 3-4 on lane_bits[0..1].

@@ -382,7 +382,6 @@ static int plan_phases(std::vector<OpT> &out, int kw, std::vector<QsvPhaseX> &ph
                 else if (op.variant == QSV_V_CTRL_DIAG1) op.variant = QSV_V_CTRL_DIAG1_SEL;
                 else if (op.variant == QSV_V_CTRL_SWAP) op.variant = QSV_V_CTRL_SWAP_SEL;
             }
-            op.oop = (uint8_t)(!C128 && qsv_op_writes_every_slot(op.slot, op.variant, op.kind, op.cls0, op.cm_c));
         }
         phases.push_back(ph);
         i = j;

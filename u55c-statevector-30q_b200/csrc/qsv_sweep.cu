@@ -13,12 +13,10 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
-#include <atomic>
 #include <cstring>
 
 #include "qsv_device.cuh"
 #include "qsv_ops.cuh"
-#include "qsv_ops_pp.cuh"
 #include "qsv_planner.h"
 #include "qsv_sweep_body.cuh"
 
@@ -46,37 +44,10 @@ struct InterpBody {
     }
 };
 
-// The interpreter in ping-pong form (qsv_ops_pp.cuh): ops that write every slot go from one register set to
-// the other, so the per-op dispatch leaves nothing to reconcile at its join. Same values.
-struct InterpBodyPP {
-    using Amp = float2;
-    static constexpr int kHalfBits = 1;
-    static constexpr bool kSmemOps = true;
-    template <int NV, int RB, int WB>
-    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane, int warp,
-                                                int bar) {
-        constexpr int NC = 1 << (5 + WB);
-        for (int ph = 0; ph < P.nphases; ph++) {
-            if (ph > 0) named_bar_sync(bar, NC);
-            const QsvPhase &Q = P.phases[ph];
-            run_phase_pp<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp, P.swz != 0);
-        }
-    }
-};
-
-template <int KW, int RB, int WB, int S, class Body>
+template <int KW, int RB, int WB, int S>
 __global__ void __launch_bounds__((1 << (5 + WB)) + 32, (KW >= 13 ? 1 : 2))
     sweep_kernel(float2 *__restrict__ state, const __grid_constant__ QsvSweep P, const __grid_constant__ CUtensorMap tmap) {
-    sweep_pipeline<KW, RB, WB, S, 1, Body>(state, P, &tmap, &g_status);
-}
-
-// the same bodies staged without a producer warp (sweep_pipeline_cd): up to 255 registers per thread with
-// 8 warps, room for the ping-pong form's two register sets
-template <int KW, int RB, int WB, int S, class Body>
-__global__ void __launch_bounds__(1 << (5 + WB), (KW >= 13 ? 1 : 2))
-    sweep_kernel_cd(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,
-                    const __grid_constant__ CUtensorMap tmap) {
-    sweep_pipeline_cd<KW, RB, WB, S, Body>(state, P, &tmap, &g_status);
+    sweep_pipeline<KW, RB, WB, S, 1, InterpBody>(state, P, &tmap, &g_status);
 }
 
 // ---------------------------------------------------------------- host launchers
@@ -117,23 +88,19 @@ cudaError_t make_tmap(CUtensorMap *map, float2 *state, const QsvSweep &sw) {
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// CD: staged by the consumers (sweep_kernel_cd, no producer warp); else by a producer warp (sweep_kernel)
-template <int KW, int RB, int WB, int S, class Body, bool CD>
+template <int KW, int RB, int WB, int S>
 static cudaError_t launch_sweep_t(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream) {
-    constexpr int NT = (1 << (5 + WB)) + (CD ? 0 : 32);
-    const size_t smem = sweep_smem_bytes<KW, S, Body>();
-    void (*kern)(float2 *, const QsvSweep, const CUtensorMap) = nullptr;
-    if constexpr (CD) kern = sweep_kernel_cd<KW, RB, WB, S, Body>;
-    else kern = sweep_kernel<KW, RB, WB, S, Body>;
+    constexpr int NT = (1 << (5 + WB)) + 32;
+    const size_t smem = sweep_smem_bytes<KW, S, InterpBody>();
     static int configured_dev = -1;     // attribute set once per device (under the engine's launch lock)
     static int per_sm = 1;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (configured_dev != dev) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(sweep_kernel<KW, RB, WB, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<KW, RB, WB, S>, NT, smem);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         configured_dev = dev;
@@ -143,23 +110,8 @@ static cudaError_t launch_sweep_t(float2 *state, const QsvSweep &sw, int nsm, cu
     if (e != cudaSuccess) return e;
     int64_t grid = (int64_t)nsm * per_sm;
     if (grid > sw.ntiles) grid = sw.ntiles;
-    kern<<<(unsigned)grid, NT, smem, stream>>>(state, sw, map);
+    sweep_kernel<KW, RB, WB, S><<<(unsigned)grid, NT, smem, stream>>>(state, sw, map);
     return cudaGetLastError();
-}
-
-template <class Body, bool CD>
-static cudaError_t launch_sweep_body(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream) {
-    int rb = 4, wb = 3;
-    layout_for_kw(sw.kw, &rb, &wb);
-    switch (sw.kw) {
-        case 13:
-            if (rb == 3) return launch_sweep_t<13, 3, 4, 3, Body, CD>(state, sw, nsm, stream);
-            return launch_sweep_t<13, 4, 3, 3, Body, CD>(state, sw, nsm, stream);
-        case 12: return launch_sweep_t<12, 4, 2, 3, Body, CD>(state, sw, nsm, stream);
-        case 11: return launch_sweep_t<11, 3, 2, 3, Body, CD>(state, sw, nsm, stream);
-        case 10: return launch_sweep_t<10, 2, 2, 3, Body, CD>(state, sw, nsm, stream);
-        default: return cudaErrorInvalidValue;
-    }
 }
 
 }  // namespace dev
@@ -188,20 +140,17 @@ cudaError_t take_device_status(int *out) {
     return cudaMemcpyToSymbol(dev::g_status, &zero, sizeof(int));
 }
 
-// Interpreter form: 1 = ping-pong register sets, staged by the consumers (default); 0 = every op in place,
-// staged by a producer warp; 2 = every op in place, staged by the consumers. Values are identical.
-static std::atomic<int> g_interp_form{1};
-
-int set_interp_form(int form) {
-    if (form < 0 || form > 2) return -1;
-    return g_interp_form.exchange(form);
-}
-
 cudaError_t launch_sweep(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream) {
-    switch (g_interp_form.load(std::memory_order_relaxed)) {
-        case 0: return dev::launch_sweep_body<dev::InterpBody, false>(state, sw, nsm, stream);
-        case 2: return dev::launch_sweep_body<dev::InterpBody, true>(state, sw, nsm, stream);
-        default: return dev::launch_sweep_body<dev::InterpBodyPP, true>(state, sw, nsm, stream);
+    int rb = 4, wb = 3;
+    layout_for_kw(sw.kw, &rb, &wb);
+    switch (sw.kw) {
+        case 13:
+            if (rb == 3) return dev::launch_sweep_t<13, 3, 4, 3>(state, sw, nsm, stream);
+            return dev::launch_sweep_t<13, 4, 3, 3>(state, sw, nsm, stream);
+        case 12: return dev::launch_sweep_t<12, 4, 2, 3>(state, sw, nsm, stream);
+        case 11: return dev::launch_sweep_t<11, 3, 2, 3>(state, sw, nsm, stream);
+        case 10: return dev::launch_sweep_t<10, 2, 2, 3>(state, sw, nsm, stream);
+        default: return cudaErrorInvalidValue;
     }
 }
 

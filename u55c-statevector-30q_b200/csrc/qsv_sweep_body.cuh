@@ -271,144 +271,5 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
     }
 }
 
-// The pipeline without a producer warp, for bodies that need more registers per thread than a block with a
-// producer warp allows: with 1 << WB consumer warps and no extra warp, each of the four schedulers holds at
-// most WB <= 3 ? 2 : 4 warps, so a thread may use up to 255 (8 warps) or 128 (16 warps) registers. Warp 0
-// issues the copies: loads of the first S tiles up front; after each tile, once every consumer has
-// finished it (block-wide barrier), the tile's store, and the load of tile j - 1 + S into the buffer of
-// tile j - 1, whose store was issued one tile earlier (so the wait for that store to have read its buffer
-// rarely stalls). Launch with 1 << (5 + WB) threads and sweep_smem_bytes<KW, S, Body, SW>() bytes of
-// dynamic shared memory. Bounded waits, the fault-injection switch and the drain on abort are those of
-// sweep_pipeline.
-template <int KW, int RB, int WB, int S, class Body, class SW = QsvSweep>
-__device__ __forceinline__ void sweep_pipeline_cd(typename Body::Amp *__restrict__ state, const SW &P,
-                                                  const CUtensorMap *tmap, int *status) {
-    using Amp = typename Body::Amp;
-    using Op = typename SW::op_type;
-    constexpr int NC = 1 << (5 + WB);        // threads (all consumers)
-    constexpr int NV = 1 << RB;
-    constexpr int TILE = 1 << KW;
-    constexpr uint32_t TILE_BYTES = (uint32_t)TILE * (uint32_t)sizeof(Amp);
-    static_assert(Body::kHalfBits + 3 + 2 + RB + WB == KW, "layout must cover the window");
-    static_assert(S >= 2, "a buffer is recycled one tile after its store");
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    Amp *bufs = reinterpret_cast<Amp *>(smem);
-    Op *sops = reinterpret_cast<Op *>(smem + ((size_t)S << KW) * sizeof(Amp));
-    __shared__ __align__(8) uint64_t full[S];
-    __shared__ volatile int abort_flag;
-
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    if (Body::kSmemOps) {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(P.ops);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(sops);
-        const int words = P.nops * (int)(sizeof(Op) / 4);
-        for (int i = tid; i < words; i += blockDim.x) dst[i] = src[i];
-    }
-    if (tid == 0) {
-        for (int f = 0; f < S; f++) mbar_init(&full[f], 1);
-        abort_flag = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    const int64_t ntiles = P.ntiles;
-    const int64_t first = blockIdx.x, stride = gridDim.x;
-    const int64_t nmine = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;
-    const uint64_t limit = wait_limit_ns(P.wait_us);
-    const bool skip_first = P.skip_load != 0 && blockIdx.x == 0;
-
-    // copies, issued by warp 0 (tile addressing as in sweep_pipeline)
-    const int lo = P.lo;
-    const int rank = P.tma_rank;
-    const int nsub = 1 << (KW - lo);
-    const uint32_t subbytes = (uint32_t)sizeof(Amp) << lo;
-    auto coords = [&](int64_t T, int32_t *c) {
-        int pos = 0;
-        for (int d = 0; d < rank; d++) {
-            const int f = P.tdim_free[d];
-            c[d] = (int32_t)(((T >> pos) & ((1ll << f) - 1)) << P.tdim_box[d]);
-            pos += f;
-        }
-    };
-    auto tile_base = [&](int64_t T) -> int64_t {
-        int64_t x = T << lo;
-        for (int i = 0; i < P.nh; i++) {
-            const int h = P.H[i];
-            x = ((x >> h) << (h + 1)) | (x & ((1ll << h) - 1));
-        }
-        return x;
-    };
-    auto sub_off = [&](int sb) -> int64_t {
-        int64_t o = 0;
-        for (int i = 0; i < KW - lo; i++)
-            if ((sb >> i) & 1) o |= 1ll << P.H[i];
-        return o;
-    };
-    auto issue_load = [&](int64_t j) {          // warp 0
-        if (skip_first && j == 0) return;
-        const int64_t T = first + j * stride;
-        const int b = (int)(j % S);
-        Amp *dst = bufs + (size_t)b * TILE;
-        if (rank) {
-            if (lane == 0) {
-                int32_t c[QSV_TMA_MAX_RANK];
-                coords(T, c);
-                mbar_arrive_expect_tx(&full[b], TILE_BYTES);
-                tma_load(dst, tmap, c, rank, &full[b]);
-            }
-            return;
-        }
-        const int64_t base = tile_base(T);
-        if (lane == 0) mbar_arrive_expect_tx(&full[b], TILE_BYTES);
-        __syncwarp();
-        for (int sb = lane; sb < nsub; sb += 32) bulk_g2s(dst + (sb << lo), state + (base | sub_off(sb)), subbytes, &full[b]);
-    };
-    auto issue_store = [&](int64_t j) {         // warp 0; every lane commits one bulk group
-        const int64_t T = first + j * stride;
-        const Amp *src = bufs + (size_t)(j % S) * TILE;
-        if (rank) {
-            if (lane == 0) {
-                int32_t c[QSV_TMA_MAX_RANK];
-                coords(T, c);
-                tma_store(tmap, c, rank, src);
-            }
-        } else {
-            const int64_t base = tile_base(T);
-            for (int sb = lane; sb < nsub; sb += 32) bulk_s2g(state + (base | sub_off(sb)), src + (sb << lo), subbytes);
-        }
-        bulk_commit();
-    };
-
-    int64_t issued = 0, j = 0;
-    if (warp == 0)
-        for (; issued < S && issued < nmine; issued++) issue_load(issued);
-    for (; j < nmine; j++) {
-        const int b = (int)(j % S);
-        if (!mbar_wait(&full[b], (uint32_t)((j / S) & 1), &abort_flag, status, limit)) break;
-        Body::template tile<NV, RB, WB>(bufs + (size_t)b * TILE, P, sops, lane, warp, 1);
-        fence_proxy_async_smem();
-        named_bar_sync(1, NC);                // every consumer's writes to buffer b are done and fenced
-        if (warp == 0) {
-            issue_store(j);
-            if (j >= 1 && j - 1 + S < nmine) {
-                bulk_wait_read_but_one();       // the store of tile j - 1 has read its buffer
-                __syncwarp();
-                issue_load(j - 1 + S);
-                issued = j + S;
-            }
-        }
-    }
-    if (warp == 0) {
-        if (j < nmine && lane == 0) {
-            // aborted: loads of tiles [j, issued) may still be in flight into this CTA's shared memory
-            for (int64_t k = j; k < issued; k++)
-                if (!(skip_first && k == 0)) mbar_wait_drain(&full[k % S], (uint32_t)((k / S) & 1), limit);
-        }
-        bulk_wait_all();
-    }
-}
-
 }  // namespace dev
 }  // namespace qsv

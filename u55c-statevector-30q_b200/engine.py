@@ -68,7 +68,6 @@ def load(path=LIB_PATH):
         "qsv_batch_launch": ([P, P, SZ, P], I32),
         "qsv_set_phase_lanes": ([ctypes.c_int], I32),
         "qsv_set_jit": ([ctypes.c_int], I32),
-        "qsv_set_interp_form": ([ctypes.c_int], I32),
         "qsv_set_wait_limit_us": ([ctypes.c_uint], I32),
         "qsv_inject_skip_load": ([ctypes.c_int], I32),
         "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
@@ -94,7 +93,7 @@ def exported_symbols():
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
             "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
-            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_interp_form", "qsv_set_wait_limit_us",
+            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_wait_limit_us",
             "qsv_inject_skip_load", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
             "qsv_jit_wait", "qsv_jit_info", "qsv_hbm_copy"]
@@ -340,7 +339,7 @@ def hbm_copy(dst, src, stream=None):
     _check(load().qsv_hbm_copy(_ptr(dst), _ptr(src), nb, _stream(stream)))
 
 
-JIT_MODES = {"off": 0, "eager": 1, "auto": 2}
+JIT_MODES = {"off": 0, "eager": 1, "auto": 2, "coarse": 3}
 
 
 def set_wait_limit_us(us):
@@ -354,19 +353,11 @@ def inject_skip_load(count=1):
     _check(load().qsv_inject_skip_load(int(count)))
 
 
-def set_interp_form(form):
-    """Interpreter sweep kernel form: 1 = ping-pong register sets (default), 0 = in place with a producer
-    warp, 2 = in place without one. Returns the previous form."""
-    rc = load().qsv_set_interp_form(int(form))
-    if rc < 0:
-        _check(rc)
-    return rc
-
-
 def set_jit(mode):
     """Specialised sweep kernels: "off" (interpreter only), "eager" (compile each new sweep structure before
-    its first launch) or "auto" (default: compile in the background once a structure's launches have swept
-    2^31 amplitudes). Values are identical in every mode. Returns the previous mode's name."""
+    its first launch), "auto" (default: compile in the background once a structure's launches have swept
+    2^31 amplitudes; meanwhile use the kernel of its coarse structure when that one is ready) or "coarse"
+    (eager, coarse structures only). Values are identical in every mode. Returns the previous mode's name."""
     rc = load().qsv_set_jit(JIT_MODES[mode] if isinstance(mode, str) else int(mode))
     if rc < 0:
         _check(rc)
@@ -389,7 +380,8 @@ def jit_wait():
 
 def jit_info():
     """Counters of the specialised-kernel cache."""
-    buf = (ctypes.c_longlong * 8)()
-    load().qsv_jit_info(ctypes.cast(buf, ctypes.c_void_p), 8)
-    keys = ["mode", "structures", "ready", "failed", "jit_launches", "interp_launches", "compile_ms", "pending"]
+    buf = (ctypes.c_longlong * 10)()
+    load().qsv_jit_info(ctypes.cast(buf, ctypes.c_void_p), 10)
+    keys = ["mode", "structures", "ready", "failed", "jit_launches", "interp_launches", "compile_ms", "pending",
+            "coarse_launches", "coarse_structures"]
     return dict(zip(keys, [int(x) for x in buf]))
