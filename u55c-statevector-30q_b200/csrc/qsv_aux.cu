@@ -17,8 +17,8 @@
 namespace qsv {
 namespace dev {
 
-#define REMAP_TB 10                 // tile bits
-#define REMAP_RUN 5                 // contiguous run bits on each side
+#define REMAP_TB 11                 // tile bits: 2^11 amplitudes per tile (2^10 for a 10-qubit state)
+#define REMAP_RUN 5                 // contiguous run bits on each side (32 amplitudes per warp access)
 #define REMAP_THREADS 256
 
 struct RemapParams {
@@ -28,58 +28,109 @@ struct RemapParams {
     uint8_t fx[40];                 // free source bits, ascending
     uint8_t fy[40];                 // destination position of free source bit fx[i]
     uint8_t ypos[REMAP_TB];         // destination position of tile source bit ubits[i]
+    int8_t swz[REMAP_TB];           // shared-memory swizzle: tile bit b >= REMAP_RUN is XORed into low bit swz[b]
 };
 
-// A = float2 (complex64) or double2 (complex128)
-template <class A>
-__global__ void __launch_bounds__(REMAP_THREADS)
+// Bit permutation of the state, one HBM read and one write per amplitude. A tile is 2^11 amplitudes that
+// share the free bits (the source bits outside the tile); it holds source bits 0..4, so a warp's 32 reads
+// are contiguous, and the source bits that land on destination bits 0..4, so a warp's 32 writes are
+// contiguous. Shared memory holds the tile as 32-bit planes (W = sizeof(A) / 4 words per amplitude) at a
+// swizzled position: a warp's stores vary tile bits 0..4 and its loads vary the tile bits of destination
+// bits 0..4; the swizzle (host-chosen, linear) moves each such bit above bit 4 onto a low bit the other
+// four leave free, so both sides hit 32 distinct banks. Each thread's tile-invariant offsets are computed
+// once; the loads of the next tile are issued before the stores of the current one.
+// (three CTAs per SM: 80 registers, three tiles of loads in flight per SM plus each CTA's next tile)
+template <class A, int TB>
+__global__ void __launch_bounds__(REMAP_THREADS, 3)
     remap_kernel(const A *__restrict__ src, A *__restrict__ dst, const __grid_constant__ RemapParams P) {
-    constexpr int TS = 1 << REMAP_TB;
-    __shared__ A tile[TS];
-    __shared__ uint64_t rd_off[TS];
-    __shared__ uint64_t wr_off[TS];
-    __shared__ uint16_t wr_pos[TS];
-    // destination-side enumeration: k's bits walk the destination positions of the tile bits, ascending,
-    // so k's low bits are destination bits 0..4 (coalesced writes)
-    uint8_t order[REMAP_TB];        // order[q] = tile bit whose destination position is the q-th smallest
+    constexpr int TS = 1 << TB;
+    constexpr int REMAP_EPT = TS / REMAP_THREADS;     // amplitudes per thread per tile
+    constexpr int W = sizeof(A) / 4;
+    using Word = uint32_t;
+    __shared__ Word plane[W * TS];
+    const int t = threadIdx.x;
+    // destination enumeration: bit q of k walks the tile bit with the q-th smallest destination position
+    uint8_t order[TB];
     {
-        bool used[REMAP_TB] = {false};
-        for (int q = 0; q < REMAP_TB; q++) {
+        bool used[TB] = {false};
+        for (int q = 0; q < TB; q++) {
             int best = -1;
-            for (int i = 0; i < REMAP_TB; i++)
+            for (int i = 0; i < TB; i++)
                 if (!used[i] && (best < 0 || P.ypos[i] < P.ypos[best])) best = i;
             used[best] = true;
             order[q] = (uint8_t)best;
         }
     }
-    for (int j = threadIdx.x; j < TS; j += REMAP_THREADS) {
+    auto swz = [&](uint32_t j) -> uint32_t {
+        uint32_t m = 0;
+        for (int b = REMAP_RUN; b < TB; b++)
+            if (P.swz[b] >= 0 && ((j >> b) & 1)) m |= 1u << P.swz[b];
+        return j ^ m;
+    };
+    uint64_t ro[REMAP_EPT], wo[REMAP_EPT];
+    uint32_t sp_in[REMAP_EPT], sp_out[REMAP_EPT];
+#pragma unroll
+    for (int e = 0; e < REMAP_EPT; e++) {
+        const uint32_t j = (uint32_t)(t + e * REMAP_THREADS);        // source-ordered tile position
         uint64_t o = 0;
-        for (int i = 0; i < REMAP_TB; i++)
+        for (int i = 0; i < TB; i++)
             if ((j >> i) & 1) o |= 1ull << P.ubits[i];
-        rd_off[j] = o;
+        ro[e] = o;
+        sp_in[e] = swz(j);
+        const uint32_t k = j;                                         // destination-ordered enumeration
         uint64_t w = 0;
         uint32_t pos = 0;
-        for (int q = 0; q < REMAP_TB; q++)
-            if ((j >> q) & 1) {
+        for (int q = 0; q < TB; q++)
+            if ((k >> q) & 1) {
                 w |= 1ull << P.ypos[order[q]];
                 pos |= 1u << order[q];
             }
-        wr_off[j] = w;
-        wr_pos[j] = (uint16_t)pos;
+        wo[e] = w;
+        sp_out[e] = swz(pos);
     }
-    __syncthreads();
+    auto bases = [&](int64_t T, uint64_t &xb, uint64_t &yb) {
+        xb = 0;
+        yb = 0;
+        for (uint64_t r = (uint64_t)T; r; r &= r - 1) {
+            const int i = __ffsll((long long)r) - 1;
+            xb |= 1ull << P.fx[i];
+            yb |= 1ull << P.fy[i];
+        }
+    };
     const int64_t ntiles = 1ll << P.nfree;
-    for (int64_t T = blockIdx.x; T < ntiles; T += gridDim.x) {
-        uint64_t xb = 0, yb = 0;
-        for (int i = 0; i < P.nfree; i++)
-            if ((T >> i) & 1) {
-                xb |= 1ull << P.fx[i];
-                yb |= 1ull << P.fy[i];
-            }
-        for (int j = threadIdx.x; j < TS; j += REMAP_THREADS) tile[j] = src[xb | rd_off[j]];
+    int64_t T = blockIdx.x;
+    if (T >= ntiles) return;
+    A v[REMAP_EPT];
+    uint64_t xb, yb;
+    bases(T, xb, yb);
+#pragma unroll
+    for (int e = 0; e < REMAP_EPT; e++) v[e] = src[xb | ro[e]];
+    while (true) {
+#pragma unroll
+        for (int e = 0; e < REMAP_EPT; e++) {
+            const Word *w = reinterpret_cast<const Word *>(&v[e]);
+#pragma unroll
+            for (int p = 0; p < W; p++) plane[p * TS + sp_in[e]] = w[p];
+        }
         __syncthreads();
-        for (int k = threadIdx.x; k < TS; k += REMAP_THREADS) dst[yb | wr_off[k]] = tile[wr_pos[k]];
-        __syncthreads();
+        const uint64_t ycur = yb;
+        const int64_t Tn = T + gridDim.x;
+        if (Tn < ntiles) {                      // next tile's loads in flight during this tile's stores
+            bases(Tn, xb, yb);
+#pragma unroll
+            for (int e = 0; e < REMAP_EPT; e++) v[e] = src[xb | ro[e]];
+        }
+#pragma unroll
+        for (int e = 0; e < REMAP_EPT; e++) {
+            A a;
+            Word *w = reinterpret_cast<Word *>(&a);
+#pragma unroll
+            for (int p = 0; p < W; p++) w[p] = plane[p * TS + sp_out[e]];
+            dst[ycur | wo[e]] = a;
+        }
+        if (Tn >= ntiles) break;
+        T = Tn;
+        __syncthreads();                        // this tile's shared-memory reads are done
     }
 }
 
@@ -284,7 +335,8 @@ cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm,
     for (int b = 0; b < REMAP_RUN; b++) { in_tile[b] = true; cnt++; }
     for (int j = 0; j < REMAP_RUN; j++)
         if (!in_tile[perm[j]]) { in_tile[perm[j]] = true; cnt++; }
-    for (int b = 0; b < n && cnt < REMAP_TB; b++)
+    const int tbits = n < REMAP_TB ? n : REMAP_TB;
+    for (int b = 0; b < n && cnt < tbits; b++)
         if (!in_tile[b]) { in_tile[b] = true; cnt++; }
     int nu = 0, nf = 0;
     for (int b = 0; b < n; b++) {
@@ -299,13 +351,34 @@ cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm,
         }
     }
     P.nfree = nf;
+    // swizzle: the tile bits carrying destination bits 0..4 vary across a warp's shared-memory loads; each of
+    // them above bit 4 is XORed onto a low bit (0..4) that none of the others occupies
+    for (int b = 0; b < REMAP_TB; b++) P.swz[b] = -1;
+    bool low_used[REMAP_RUN] = {false};
+    int hi[REMAP_RUN], nhi = 0;
+    for (int j = 0; j < REMAP_RUN; j++) {
+        int tb = -1;
+        for (int i = 0; i < nu; i++)
+            if (P.ubits[i] == perm[j]) tb = i;
+        if (tb < REMAP_RUN) low_used[tb] = true;
+        else hi[nhi++] = tb;
+    }
+    for (int h = 0, slot = 0; h < nhi; h++) {
+        while (low_used[slot]) slot++;
+        P.swz[hi[h]] = (int8_t)slot;
+        low_used[slot] = true;
+    }
     const int64_t ntiles = 1ll << nf;
-    int64_t grid = (int64_t)nsm * 8;
+    int64_t grid = (int64_t)nsm * 3;
     if (grid > ntiles) grid = ntiles;
-    if (dtype)
-        dev::remap_kernel<double2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const double2 *)src, (double2 *)dst, P);
-    else
-        dev::remap_kernel<float2><<<(unsigned)grid, REMAP_THREADS, 0, stream>>>((const float2 *)src, (float2 *)dst, P);
+    const unsigned g = (unsigned)grid;
+    if (tbits == REMAP_TB) {
+        if (dtype) dev::remap_kernel<double2, REMAP_TB><<<g, REMAP_THREADS, 0, stream>>>((const double2 *)src, (double2 *)dst, P);
+        else dev::remap_kernel<float2, REMAP_TB><<<g, REMAP_THREADS, 0, stream>>>((const float2 *)src, (float2 *)dst, P);
+    } else {                                  // a 10-qubit state is one tile of 2^10
+        if (dtype) dev::remap_kernel<double2, 10><<<g, REMAP_THREADS, 0, stream>>>((const double2 *)src, (double2 *)dst, P);
+        else dev::remap_kernel<float2, 10><<<g, REMAP_THREADS, 0, stream>>>((const float2 *)src, (float2 *)dst, P);
+    }
     return cudaGetLastError();
 }
 
