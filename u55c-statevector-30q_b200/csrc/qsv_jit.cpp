@@ -98,16 +98,6 @@ int interleave_for(const QsvSweep &sw, int groups) {
     return mode == 2 || sw.tma_rank > 0 ? 1 : 0;
 }
 
-// Whether dense register-bit ops read pre-splatted coefficients (QsvSweepT::csp) instead of building the
-// (c, c) pairs of the packed FP32x2 arithmetic from scalars in the kernel. QSV_JIT_SPLAT=0 or 1 forces it.
-bool splat_enabled() {
-    static const int v = [] {
-        const char *e = std::getenv("QSV_JIT_SPLAT");
-        return e ? std::atoi(e) : 1;
-    }();
-    return v != 0;
-}
-
 struct Drv {
     PFN_cuModuleLoadData_v2000 module_load = nullptr;
     PFN_cuModuleGetFunction_v2000 get_function = nullptr;
@@ -205,7 +195,7 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
     std::string k;
     auto put = [&](int v) { k.push_back((char)(v & 0xff)); };
     auto put32 = [&](uint32_t v) { k.append(reinterpret_cast<const char *>(&v), 4); };
-    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops); put(sw.swz); put(splat_enabled());
+    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops); put(sw.swz);
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
         for (int r = 0; r < rb; r++) put(ph.reg_bits[r]);
@@ -225,7 +215,6 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
 // CUDA source of the kernel specialised to sw's structure
 std::string gen_source(const QsvSweep &sw, int rb, int wb) {
     const int groups = groups_for(sw, wb);
-    const bool splat = splat_enabled();
     const int nc = 1 << (5 + wb), nt = groups * nc + 32, minb = sw.kw >= 13 ? 1 : 2;
     std::ostringstream s;
     s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
@@ -266,10 +255,6 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
             else if (op.slot < QSV_SLOT_LANE0 && op.variant == QSV_V_MUX)
                 s << "            jit_reg_mux<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << mux << ">(R, I, P.ops[" << o
                   << "], tb);\n";
-            else if (op.slot < QSV_SLOT_LANE0 && splat &&
-                     (var == QSV_V_UNI_DENSE || var == QSV_V_UNI_DENSE_R0 || var == QSV_V_CTRL_DENSE))
-                s << "            jit_reg_s<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
-                  << ">(R, I, P.csp[" << o << "], tb);\n";
             else if (op.slot < QSV_SLOT_LANE0)
                 s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb);\n";

@@ -59,64 +59,6 @@ __device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float
     }
 }
 
-// dense2 / dense2_r0 (qsv_ops.cuh) with the host's pre-splatted coefficients (QsvSweepT::csp, read from the
-// parameter block): the same chains, term for term, with no pair built from a scalar at run time
-__device__ __forceinline__ float2 f2s(const float2s &c) { return make_float2(c.x, c.y); }
-__device__ __forceinline__ void dense2s(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float2s *c) {
-    float2 t, u;
-    t = __fmul2_rn(f2s(c[QSV_SPLAT_NM3]), I1); t = __ffma2_rn(f2s(c[QSV_SPLAT_M2]), R1, t);
-    t = __ffma2_rn(f2s(c[QSV_SPLAT_NM1]), I0, t);
-    const float2 y0r = __ffma2_rn(f2s(c[QSV_SPLAT_M0]), R0, t);
-    u = __fmul2_rn(f2s(c[QSV_SPLAT_M3]), R1); u = __ffma2_rn(f2s(c[QSV_SPLAT_M2]), I1, u);
-    u = __ffma2_rn(f2s(c[QSV_SPLAT_M1]), R0, u);
-    const float2 y0i = __ffma2_rn(f2s(c[QSV_SPLAT_M0]), I0, u);
-    t = __fmul2_rn(f2s(c[QSV_SPLAT_NM5]), I0); t = __ffma2_rn(f2s(c[QSV_SPLAT_M4]), R0, t);
-    t = __ffma2_rn(f2s(c[QSV_SPLAT_NM7]), I1, t);
-    const float2 y1r = __ffma2_rn(f2s(c[QSV_SPLAT_M6]), R1, t);
-    u = __fmul2_rn(f2s(c[QSV_SPLAT_M5]), R0); u = __ffma2_rn(f2s(c[QSV_SPLAT_M4]), I0, u);
-    u = __ffma2_rn(f2s(c[QSV_SPLAT_M7]), R1, u);
-    const float2 y1i = __ffma2_rn(f2s(c[QSV_SPLAT_M6]), I1, u);
-    R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
-}
-__device__ __forceinline__ void dense2s_r0(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float2s *c) {
-    float2 t, u;
-    t = __fmul2_rn(f2s(c[QSV_SPLAT_NM3]), I1); t = __ffma2_rn(f2s(c[QSV_SPLAT_M2]), R1, t);
-    const float2 y0r = __ffma2_rn(f2s(c[QSV_SPLAT_M0]), R0, t);
-    u = __fmul2_rn(f2s(c[QSV_SPLAT_M3]), R1); u = __ffma2_rn(f2s(c[QSV_SPLAT_M2]), I1, u);
-    const float2 y0i = __ffma2_rn(f2s(c[QSV_SPLAT_M0]), I0, u);
-    t = __fmul2_rn(f2s(c[QSV_SPLAT_NM5]), I0); t = __ffma2_rn(f2s(c[QSV_SPLAT_M4]), R0, t);
-    t = __ffma2_rn(f2s(c[QSV_SPLAT_NM7]), I1, t);
-    const float2 y1r = __ffma2_rn(f2s(c[QSV_SPLAT_M6]), R1, t);
-    u = __fmul2_rn(f2s(c[QSV_SPLAT_M5]), R0); u = __ffma2_rn(f2s(c[QSV_SPLAT_M4]), I0, u);
-    u = __ffma2_rn(f2s(c[QSV_SPLAT_M7]), R1, u);
-    const float2 y1i = __ffma2_rn(f2s(c[QSV_SPLAT_M6]), I1, u);
-    R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
-}
-
-// register-bit dense ops with pre-splatted coefficients: uniform (VAR QSV_V_UNI_DENSE / _R0) or controlled
-// (QSV_V_CTRL_DENSE) -- jit_reg's forms with dense2s in place of dense2
-template <int NV, int RBIT, int VAR, int CMREG, uint32_t CMTHR>
-__device__ __forceinline__ void jit_reg_s(float2 (&R)[NV], float2 (&I)[NV], const float2s *cs, uint32_t tb) {
-    constexpr int B = 1 << RBIT;
-    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
-    if constexpr (VAR == QSV_V_UNI_DENSE) {
-#pragma unroll
-        for (int r = 0; r < NV; r++)
-            if (!(r & B)) dense2s(R[r], I[r], R[r | B], I[r | B], cs);
-    } else if constexpr (VAR == QSV_V_UNI_DENSE_R0) {
-#pragma unroll
-        for (int r = 0; r < NV; r++)
-            if (!(r & B)) dense2s_r0(R[r], I[r], R[r | B], I[r | B], cs);
-    } else {
-        static_assert(VAR == QSV_V_CTRL_DENSE, "pre-splatted forms: dense variants only");
-        if (tok) {
-#pragma unroll
-            for (int r = 0; r < NV; r++)
-                if (!(r & B) && (r & CMREG) == CMREG) dense2s(R[r], I[r], R[r | B], I[r | B], cs);
-        }
-    }
-}
-
 __device__ __forceinline__ void jit_mat(float (&m)[8], const float *src) {
 #pragma unroll
     for (int e = 0; e < 8; e++) m[e] = src[e];

@@ -121,23 +121,6 @@ struct QsvOpD {
     uint8_t pad[6];
 };
 
-// a (c, c) coefficient pair; plain struct so that host code and NVRTC need no CUDA vector types
-struct alignas(8) float2s {
-    float x, y;
-};
-// positions in QsvSweepT::csp[o]: m = the op's matrix as (re, im) x 4
-#define QSV_SPLAT_M0 0          // m[0]
-#define QSV_SPLAT_M1 1          // m[1]
-#define QSV_SPLAT_NM1 2         // -m[1]
-#define QSV_SPLAT_M2 3
-#define QSV_SPLAT_M3 4
-#define QSV_SPLAT_NM3 5
-#define QSV_SPLAT_M4 6
-#define QSV_SPLAT_M5 7
-#define QSV_SPLAT_NM5 8
-#define QSV_SPLAT_M6 9
-#define QSV_SPLAT_M7 10
-#define QSV_SPLAT_NM7 11
 
 // A phase's thread layout: lane bits 0-2 sit on tile bits lane_lo[0..2] (1, 2, 3 for complex64 unless the
 // sweep is swizzled, see QsvSweepT::swz; 0, 1, 2 for complex128), lane bits 3-4 on lane_bits[0..1].
@@ -183,10 +166,6 @@ struct QsvSweepT {
     int32_t skip_load;          // fault injection for tests: 1 = block 0 never loads its first tile (0: off)
     QsvPhase phases[QSV_MAX_PHASES];
     OpT ops[QSV_MAX_SWEEP_OPS];
-    // complex64 sweeps: each op's dense matrix (M0 for uniform ops, M1 otherwise) with every real coefficient
-    // as a (c, c) pair, negated copies included (QSV_SPLAT_*), so a specialised kernel's packed FP32x2
-    // arithmetic reads its operands straight from the parameter block (complex128 sweeps leave it zero)
-    float2s csp[QSV_MAX_SWEEP_OPS][12];
 };
 typedef QsvSweepT<QsvOp> QsvSweep;      // complex64 state, fp32 matrices
 typedef QsvSweepT<QsvOpD> QsvSweepD;    // complex128 state, fp64 matrices

@@ -469,15 +469,6 @@ static int fill_sweep(const std::vector<PhysOp> &ops, size_t b, size_t e, uint64
     sw.nops = (int)vops.size();
     sw.nphases = (int)vph.size();
     std::memcpy(sw.ops, vops.data(), vops.size() * sizeof(OpT));
-    if (!C128) {
-        for (size_t o = 0; o < vops.size(); o++) {
-            const OpT &op = vops[o];
-            float m[8];
-            for (int e = 0; e < 8; e++) m[e] = (float)(op.kind == QSV_K_UNI ? op.m0[e] : op.m1[e]);
-            const float v[12] = {m[0], m[1], -m[1], m[2], m[3], -m[3], m[4], m[5], -m[5], m[6], m[7], -m[7]};
-            for (int k = 0; k < 12; k++) sw.csp[o][k] = float2s{v[k], v[k]};
-        }
-    }
     for (size_t p = 0; p < vph.size(); p++) {
         QsvPhase &d = sw.phases[p];
         const QsvPhaseX &x = vph[p];
