@@ -180,7 +180,7 @@ QSV_API int qsv_set_phase_lanes(int k);
  * 2 = automatic (default): a structure is compiled in background threads once its launches have swept
  * 2^31 amplitudes in total (two sweeps of a 30-qubit state, 512 of a 22-qubit one; at most 64 compilations
  * wait at a time), and used from the first launch after its kernel is ready; until then the sweep runs its
- * coarse structure's kernel, compiled by the same rule over the work of all sweeps sharing it, or the
+ * coarse structure's kernel, compiled once the sweeps sharing it have swept 2^30 amplitudes, or the
  * interpreter; 3 = eager with coarse structures only. Switching to mode 0 drops waiting compilations and
  * waits for running ones. Returns the previous mode. Process-wide. */
 QSV_API int qsv_set_jit(int mode);

@@ -24,8 +24,8 @@
 // have swept add up to kWorkThreshold (a compilation costs about a second of one host core, worth it
 // for sweeps that run often or over large states), with at most kMaxQueued compilations waiting; until
 // then a sweep runs the kernel of its coarse structure, compiled by the same rule with the work of every
-// sweep that shares it (kCoarseThreshold), or the interpreter; 3 = eager, coarse structures only (tests
-// and measurements of the coarse kernels).
+// sweep that shares it (kCoarseThreshold, 2^30 amplitudes), or the interpreter; 3 = eager, coarse
+// structures only (tests and measurements of the coarse kernels).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -57,7 +57,9 @@ cudaError_t status_word_ptr(int **out);
 namespace {
 
 constexpr double kWorkThreshold = 2147483648.0;   // 2^31 amplitudes: 2 sweeps at 30 qubits, 512 at 22
-constexpr double kCoarseThreshold = 2147483648.0; // the same amount, summed over the sweeps of a coarse key
+constexpr double kCoarseThreshold = 1073741824.0; // 2^30, summed over the sweeps of a coarse key: a coarse
+                                                  // kernel serves many sweeps, so it is worth compiling once
+                                                  // one 30-qubit sweep (or 64 at 24 qubits) has used it
 constexpr size_t kMaxQueued = 64;
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
