@@ -84,7 +84,8 @@ __global__ void __launch_bounds__((1 << (5 + WB)) + 32, (KW >= 13 ? 1 : 2))
         for (int ph = it.ph_begin; ph < it.ph_end; ph++) {
             if (ph > it.ph_begin) named_bar_sync(1, NC);
             const QsvPhaseX &Q = phases[ph];
-            run_phase<NV, RB, WB>(tile, Q, ops, Q.op_begin, Q.op_end, lane, warp);
+            run_phase<NV, RB, WB>(tile, Q, ops, Q.op_begin, Q.op_end, lane, warp, false, ph > it.ph_begin,
+                                  ph + 1 < it.ph_end);
         }
         fence_proxy_async_smem();
         mbar_arrive(&done[b]);

@@ -239,7 +239,8 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
         s << ";\n            float2 R[NV], I[NV];\n";
         std::string rbits;
         for (int r = 0; r < rb; r++) rbits += (r ? ", " : "") + std::to_string((int)ph.reg_bits[r]);
-        s << "            jit_load<NV, " << (int)sw.swz << ", " << rbits << ">(tile, tb, R, I);\n";
+        s << "            jit_load<NV, " << (int)sw.swz << ", " << (p > 0 ? 1 : 0) << ", " << rbits
+          << ">(tile, tb, R, I);\n";
         for (int o = ph.op_begin; o < ph.op_end; o++) {
             const QsvOp &op = sw.ops[o];
             const std::string thr = std::to_string(op.cm_thr) + "u";
@@ -267,7 +268,8 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
                 s << "            jit_lane<NV, " << (op.slot - QSV_SLOT_LANE0) << ", " << (int)op.variant << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb, lane);\n";
         }
-        s << "            jit_store<NV, " << (int)sw.swz << ", " << rbits << ">(tile, tb, R, I);\n            break;\n        }\n";
+        s << "            jit_store<NV, " << (int)sw.swz << ", " << (p + 1 < sw.nphases ? 1 : 0) << ", " << rbits
+          << ">(tile, tb, R, I);\n            break;\n        }\n";
     }
     s << "        default: break;\n        }\n    }\n"
       << "    template <int NV, int RB, int WB>\n"

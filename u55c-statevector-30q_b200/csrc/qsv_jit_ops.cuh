@@ -36,26 +36,29 @@ __device__ __forceinline__ constexpr uint32_t jit_reg_off(int r) {
 }
 
 // SWZ: the tile is stored with the 128-byte swizzle (swz128); the thread base and the register offsets
-// (disjoint bits) are swizzled separately and combined with XOR, the offsets at compile time
-template <int NV, int SWZ, int... RBITS>
+// (disjoint bits) are swizzled separately and combined with XOR, the offsets at compile time.
+// SPLIT: the 16-byte slot holds (re0, re1, im0, im1) -- the in-tile order between two phases of a tile,
+// which loads and stores straight into the (re, re) / (im, im) register pairs -- instead of the state's
+// interleaved (re0, im0, re1, im1), which the first phase reads and the last phase writes.
+template <int NV, int SWZ, int SPLIT, int... RBITS>
 __device__ __forceinline__ void jit_load(const float2 *tile, uint32_t tb, float2 (&R)[NV], float2 (&I)[NV]) {
     const uint32_t base = SWZ ? swz128(tb) : tb;
 #pragma unroll
     for (int r = 0; r < NV; r++) {
         const uint32_t off = jit_reg_off<RBITS...>(r);
         const float4 v = *reinterpret_cast<const float4 *>(tile + (base ^ (SWZ ? swz128(off) : off)));
-        R[r] = make_float2(v.x, v.z);
-        I[r] = make_float2(v.y, v.w);
+        R[r] = SPLIT ? make_float2(v.x, v.y) : make_float2(v.x, v.z);
+        I[r] = SPLIT ? make_float2(v.z, v.w) : make_float2(v.y, v.w);
     }
 }
-template <int NV, int SWZ, int... RBITS>
+template <int NV, int SWZ, int SPLIT, int... RBITS>
 __device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float2 (&R)[NV], const float2 (&I)[NV]) {
     const uint32_t base = SWZ ? swz128(tb) : tb;
 #pragma unroll
     for (int r = 0; r < NV; r++) {
         const uint32_t off = jit_reg_off<RBITS...>(r);
         *reinterpret_cast<float4 *>(tile + (base ^ (SWZ ? swz128(off) : off))) =
-            make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+            SPLIT ? make_float4(R[r].x, R[r].y, I[r].x, I[r].y) : make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
     }
 }
 

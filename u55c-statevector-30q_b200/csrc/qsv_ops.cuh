@@ -449,10 +449,13 @@ __device__ __forceinline__ uint32_t swz128(uint32_t x) { return x ^ ((x >> 3) & 
 
 // One phase of a tile in shared memory: read the thread's 2^RB float4 in the phase's layout, apply ops
 // [op_begin, op_end), write them back. PH is any phase record with reg_bits / lane_lo / lane_bits /
-// warp_bits; swz: the tile is stored swizzled.
+// warp_bits; swz: the tile is stored swizzled. split_in / split_out: the slots hold (re0, re1, im0, im1),
+// the in-tile order between two phases (no repacking into the register pairs), instead of the state's
+// interleaved order (first phase in, last phase out).
 template <int NV, int RB, int WB, class PH>
 __device__ __forceinline__ void run_phase(float2 *tile, const PH &Q, const QsvOp *ops, int op_begin, int op_end,
-                                          int lane, int warp, bool swz = false) {
+                                          int lane, int warp, bool swz = false, bool split_in = false,
+                                          bool split_out = false) {
     uint32_t tb = ((uint32_t)(lane & 1) << Q.lane_lo[0]) | ((uint32_t)((lane >> 1) & 1) << Q.lane_lo[1]) |
                   ((uint32_t)((lane >> 2) & 1) << Q.lane_lo[2]) | ((uint32_t)((lane >> 3) & 1) << Q.lane_bits[0]) |
                   ((uint32_t)((lane >> 4) & 1) << Q.lane_bits[1]);
@@ -470,16 +473,31 @@ __device__ __forceinline__ void run_phase(float2 *tile, const PH &Q, const QsvOp
     };
     auto addr = [&](int r) -> uint32_t { return swz ? swz128(pos(r)) : pos(r); };
     float2 R[NV], I[NV];
+    if (split_in) {
 #pragma unroll
-    for (int r = 0; r < NV; r++) {
-        const float4 v = *reinterpret_cast<const float4 *>(tile + addr(r));
-        R[r] = make_float2(v.x, v.z);
-        I[r] = make_float2(v.y, v.w);
+        for (int r = 0; r < NV; r++) {
+            const float4 v = *reinterpret_cast<const float4 *>(tile + addr(r));
+            R[r] = make_float2(v.x, v.y);
+            I[r] = make_float2(v.z, v.w);
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < NV; r++) {
+            const float4 v = *reinterpret_cast<const float4 *>(tile + addr(r));
+            R[r] = make_float2(v.x, v.z);
+            I[r] = make_float2(v.y, v.w);
+        }
     }
     for (int o = op_begin; o < op_end; o++) apply_op<NV, RB>(ops[o], R, I, tb, lane);
+    if (split_out) {
 #pragma unroll
-    for (int r = 0; r < NV; r++)
-        *reinterpret_cast<float4 *>(tile + addr(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+        for (int r = 0; r < NV; r++)
+            *reinterpret_cast<float4 *>(tile + addr(r)) = make_float4(R[r].x, R[r].y, I[r].x, I[r].y);
+    } else {
+#pragma unroll
+        for (int r = 0; r < NV; r++)
+            *reinterpret_cast<float4 *>(tile + addr(r)) = make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+    }
 }
 
 }  // namespace dev

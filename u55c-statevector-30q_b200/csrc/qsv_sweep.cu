@@ -39,7 +39,8 @@ struct InterpBody {
         for (int ph = 0; ph < P.nphases; ph++) {
             if (ph > 0) named_bar_sync(bar, NC);
             const QsvPhase &Q = P.phases[ph];
-            run_phase<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp, P.swz != 0);
+            run_phase<NV, RB, WB>(tile, Q, sops, Q.op_begin, Q.op_end, lane, warp, P.swz != 0, ph > 0,
+                                  ph + 1 < P.nphases);
         }
     }
 };
