@@ -61,6 +61,7 @@ constexpr double kCoarseThreshold = 1073741824.0; // 2^30, summed over the sweep
                                                   // kernel serves many sweeps, so it is worth compiling once
                                                   // one 30-qubit sweep (or 64 at 24 qubits) has used it
 constexpr size_t kMaxQueued = 64;
+constexpr size_t kMaxEntries = 8192;   // structures tracked; past it, the ones never queued are forgotten
 constexpr int kMaxDevices = 64;
 constexpr int kStages = 3;         // tile buffers in flight (as the interpreter)
 
@@ -415,6 +416,14 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, b
     const std::string key = (coarse ? "C" : "E") + key_of(sw, rb, wb);
     auto it = j.map.find(key);
     if (it != j.map.end()) return it->second;
+    if (j.map.size() >= kMaxEntries) {
+        // a long-running process that meets many one-off structures: drop the ones that were never queued
+        // (their work counts restart); queued, compiled and failed ones stay
+        for (auto m = j.map.begin(); m != j.map.end();) {
+            if (m->second->state == kNew && m->second.use_count() == 1) m = j.map.erase(m);
+            else ++m;
+        }
+    }
     auto e = std::make_shared<Entry>();
     e->kw = sw.kw;
     e->rb = rb;
