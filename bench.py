@@ -229,6 +229,14 @@ def batched_main(a):
     t0 = time.perf_counter()
     progs = batch.compile_many(circs, pool=cpool)
     t_compile = time.perf_counter() - t0
+    # algorithmic bytes of one batch: a circuit of at most 13 qubits runs whole in shared memory (one read
+    # and one write of its state), a larger one sweeps its state once per engine sweep (16 B per amplitude)
+    work_bytes = 0
+    for qc, (prog, fmap, n, npass) in zip(circs, progs):
+        if n <= batch.SMALL_MAX:
+            work_bytes += 16 << n
+        else:
+            work_bytes += sum(len(engine.plan_segment(seg, n)) for kind, seg in prog if kind == "segment") * (16 << n)
     br = batch.BatchRunner(streams=8, autotune=True)
     plan = br.prepare(circs, programs=progs)
     br.capture(plan)
@@ -276,6 +284,7 @@ def batched_main(a):
                                      "batched_circuits_per_s": count / t_e2e_b,
                                      "note": "new batch from circuits: compile in a running worker pool + plan + one pass, vs "
                                              "compile and run one circuit at a time"},
+                      "algorithmic_bytes": work_bytes, "hbm_floor_s": work_bytes / (_peaks()[0] * 1e9),
                       "graph_launches": plan.launches, "host_compile_s": t_compile,
                       "specialised_kernels": engine.jit_info(), "clocks": clk.summary()}))
 
