@@ -114,9 +114,16 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(pkg, n, depth, seed, k=12, max_high=4):
+def workload(pkg, n, depth, seed, k=12, max_high=4, family="random_layer"):
+    """The benchmark circuit (random_layer: the headline) or, for profiling other sweep mixes through the
+    same timing path, one of the reference's families (rqc with `depth` layers, vqe, qft)."""
     gen = pkg.generators
-    qc = gen.random_layer(n, depth, seed)
+    if family == "random_layer":
+        qc = gen.random_layer(n, depth, seed)
+    elif family == "rqc":
+        qc = gen.rqc(n, depth, seed)
+    else:
+        qc = getattr(gen, family)(n)
     prog, fmap, stats = pkg.compile_circuit(qc, n, k, max_high=max_high)
     return qc, prog, fmap, stats
 
@@ -495,8 +502,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the complex128 (FP64) comparison runs")
-    ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off"],
-                    help="specialised sweep kernels (compiled before the warm-up unless off)")
+    ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off", "coarse"],
+                    help="specialised sweep kernels (compiled before the warm-up unless off; coarse: kernels of "
+                         "coarse sweep structures only)")
+    ap.add_argument("--family", default="random_layer", choices=["random_layer", "rqc", "vqe", "qft"],
+                    help="rl30 workload circuit: the headline random-layer circuit (default) or, for profiles, "
+                         "a reference family")
     ap.add_argument("--workload", default="rl30", choices=["rl30", "precision", "batched", "served", "latency", "families"],
                     help="rl30: the headline sweep benchmark; precision: the complex64 / complex128 study "
                          "(33 qubits complex64, 32 qubits complex128 vs complex64); batched: 512 circuits of "
@@ -525,9 +536,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pkg = _package()
-    qc, prog, fmap, stats = workload(pkg, a.n, a.depth, a.seed)
+    qc, prog, fmap, stats = workload(pkg, a.n, a.depth, a.seed, family=a.family)
     segs = [p for kind, p in prog if kind == "segment"]
-    cfg = {"workload": f"random_layer n={a.n} depth={a.depth} seed={a.seed}, complex64 ({8 << a.n >> 30} GiB "
+    shape = (f"{a.family} n={a.n} depth={a.depth} seed={a.seed}" if a.family in ("random_layer", "rqc")
+             else f"{a.family} n={a.n}")
+    cfg = {"workload": f"{shape}, complex64 ({8 << a.n >> 30} GiB "
                        f"state), QSV2 k=12 M=4 from the reference scheduler",
            "n_qubits": a.n, "depth": a.depth, "qsv2_passes": stats.n_passes, "ops": stats.n_ops,
            "l2": "inputs larger than L2 (8 GiB state vs 126 MB), no flush", "parallelism": f"replicas x{a.gpus}"}
