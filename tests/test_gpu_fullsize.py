@@ -124,3 +124,47 @@ def test_accuracy_vs_fp64_30q(torch, name):
     assert m["one_minus_f"] <= 1e-5, m
     assert m["max_abs_err"] <= 1e-6, m
     assert abs(m["norm"] - 1) <= 1e-4, m
+
+
+@pytest.mark.timeout(1200)
+def test_exact_vs_oracle_28q(torch):
+    """Value for value against the C oracle near the headline size: random-layer 28 qubits (2 GiB), depth 4,
+    seed 1, through the specialised kernels (the headline's kernels) and the interpreter."""
+    from oracle import oracle as orc
+    n = 28
+    qc = gen.random_layer(n, 4, 1)
+    prog, fmap, _ = q.compile_circuit(qc, n, 12)
+    ref = np.zeros(1 << n, dtype=np.complex64)
+    ref[0] = 1
+    for kind, seg in prog:
+        ref = orc.run_segment(ref, seg)
+    for mode in ("eager", "off"):
+        st, _ = _run(torch, qc, n, jit=mode)
+        got = st.cpu().numpy()
+        del st
+        torch.cuda.empty_cache()
+        assert np.array_equal(got, ref), mode
+
+
+@pytest.mark.timeout(900)
+def test_config1_exact_vs_oracle_and_golden_model(torch):
+    """Config 1 at its own size: 20 qubits, complex64, 20 random layers (U3 + CX brickwork), seed 0, compiled
+    by the reference scheduler (k = 12, M = 4): exact against the C oracle, within 2e-6 per amplitude of the
+    reference's numpy golden model (host/sv/model.py, restated in oracle/golden_model.py), and 1 - F <= 1e-5
+    against the dense FP64 statevector."""
+    from oracle import golden_model as gm
+    from oracle import oracle as orc
+    n = 20
+    qc = gen.random_layer(n, 20, 0)
+    prog, fmap, _ = q.compile_circuit(qc, n, 12)
+    ref = np.zeros(1 << n, dtype=np.complex64)
+    ref[0] = 1
+    for kind, seg in prog:
+        ref = orc.run_segment(ref, seg)
+    st, _ = _run(torch, qc, n, jit="auto")
+    got = st.cpu().numpy()
+    assert np.array_equal(got, ref)
+    golden = gm.run_program(prog, n, 1, list(range(n)))
+    assert np.max(np.abs(got - golden)) <= 2e-6
+    m = orc.metrics(orc.statevector_f64(qc), orc.unpermute(got, fmap))
+    assert m["one_minus_f"] <= 1e-5
