@@ -486,7 +486,7 @@ def families_main(a):
                       "value": statistics.median(o["sweep_gbs"] for o in out), "unit": "GB/s (median sweep_gbs)",
                       "higher_is_better": True, "n_gpus": 1, "dtype": "c64 (fp32 arithmetic)",
                       "data": "synthetic (seeded circuits)", "config": {"workload": f"ghz, qft, rqc d10, vqe L2 at n={n}"},
-                      "peak_gbs": _peaks()[0], "circuits": out}))
+                      "peak_gbs": _peaks()[0], "circuits": out, "specialised_kernels": engine.jit_info()}))
 
 
 # ------------------------------------------------------------------ main
