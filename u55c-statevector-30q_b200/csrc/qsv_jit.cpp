@@ -101,17 +101,6 @@ int interleave_for(const QsvSweep &sw, int groups) {
     return mode == 2 || sw.tma_rank > 0 ? 1 : 0;
 }
 
-// Whether dense register-bit ops read (c, c) coefficient pairs from a shared-memory table built by each CTA
-// (one shared-memory load per pair) instead of building the pairs from scalars in registers.
-// QSV_JIT_SMEMCOEF=0 or 1 forces it.
-bool smem_coef_enabled() {
-    static const int v = [] {
-        const char *e = std::getenv("QSV_JIT_SMEMCOEF");
-        return e ? std::atoi(e) : 0;
-    }();
-    return v != 0;
-}
-
 struct Drv {
     PFN_cuModuleLoadData_v2000 module_load = nullptr;
     PFN_cuModuleGetFunction_v2000 get_function = nullptr;
@@ -209,7 +198,7 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
     std::string k;
     auto put = [&](int v) { k.push_back((char)(v & 0xff)); };
     auto put32 = [&](uint32_t v) { k.append(reinterpret_cast<const char *>(&v), 4); };
-    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops); put(sw.swz); put(smem_coef_enabled());
+    put(sw.kw); put(rb); put(wb); put(sw.nphases); put(sw.nops); put(sw.swz);
     for (int p = 0; p < sw.nphases; p++) {
         const QsvPhase &ph = sw.phases[p];
         for (int r = 0; r < rb; r++) put(ph.reg_bits[r]);
@@ -229,7 +218,6 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
 // CUDA source of the kernel specialised to sw's structure
 std::string gen_source(const QsvSweep &sw, int rb, int wb) {
     const int groups = groups_for(sw, wb);
-    const bool scoef = smem_coef_enabled();
     const int nc = 1 << (5 + wb), nt = groups * nc + 32, minb = sw.kw >= 13 ? 1 : 2;
     std::ostringstream s;
     s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_jit_ops.cuh\"\n"
@@ -237,11 +225,10 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
       << "    using Amp = float2;\n"
       << "    static constexpr int kHalfBits = 1;\n"
       << "    static constexpr bool kSmemOps = false;\n"
-      << "    static constexpr bool kSmemCoef = " << (scoef ? "true" : "false") << ";\n"
       << "    static constexpr int kPhases = " << sw.nphases << ";\n"
       << "    // one phase of a tile: load in the phase's layout, apply its ops, store\n"
       << "    template <int NV, int RB, int WB>\n"
-      << "    static __device__ __forceinline__ void phase(int p, float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane,\n"
+      << "    static __device__ __forceinline__ void phase(int p, float2 *tile, const QsvSweep &P, const QsvOp *, int lane,\n"
       << "                                                 int warp) {\n"
       << "        switch (p) {\n";
     for (int p = 0; p < sw.nphases; p++) {
@@ -272,10 +259,6 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
             else if (op.slot < QSV_SLOT_LANE0 && op.variant == QSV_V_MUX)
                 s << "            jit_reg_mux<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << mux << ">(R, I, P.ops[" << o
                   << "], tb);\n";
-            else if (op.slot < QSV_SLOT_LANE0 && scoef &&
-                     (var == QSV_V_UNI_DENSE || var == QSV_V_UNI_DENSE_R0 || var == QSV_V_CTRL_DENSE))
-                s << "            jit_reg_c<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
-                  << ">(R, I, reinterpret_cast<const float2 *>(sops) + " << o * 12 << ", tb);\n";
             else if (op.slot < QSV_SLOT_LANE0)
                 s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb);\n";
@@ -563,8 +546,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
     const int NT = e->groups * (1 << (5 + wb)) + 32;
     // sweep_smem_bytes of the generated body: the tile buffers plus 1 KiB for their 1024-byte alignment
-    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN +
-                        (smem_coef_enabled() ? sizeof(float2) * QSV_COEF_PAIRS * QSV_MAX_SWEEP_OPS : 0);
+    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN;
     if (!e->fn[dev]) {
         // loading a module is not a stream operation: keep it out of stream captures
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;

@@ -62,56 +62,6 @@ __device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float
     }
 }
 
-// dense2 / dense2_r0 (qsv_ops.cuh) with the (c, c) coefficient pairs read from the kernel's shared-memory
-// coefficient table (sweep_pipeline, Body::kSmemCoef): the same chains, term for term
-__device__ __forceinline__ void dense2c(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float2 *c) {
-    float2 t, u;
-    t = __fmul2_rn(c[QSV_COEF_NM3], I1); t = __ffma2_rn(c[QSV_COEF_M2], R1, t); t = __ffma2_rn(c[QSV_COEF_NM1], I0, t);
-    const float2 y0r = __ffma2_rn(c[QSV_COEF_M0], R0, t);
-    u = __fmul2_rn(c[QSV_COEF_M3], R1); u = __ffma2_rn(c[QSV_COEF_M2], I1, u); u = __ffma2_rn(c[QSV_COEF_M1], R0, u);
-    const float2 y0i = __ffma2_rn(c[QSV_COEF_M0], I0, u);
-    t = __fmul2_rn(c[QSV_COEF_NM5], I0); t = __ffma2_rn(c[QSV_COEF_M4], R0, t); t = __ffma2_rn(c[QSV_COEF_NM7], I1, t);
-    const float2 y1r = __ffma2_rn(c[QSV_COEF_M6], R1, t);
-    u = __fmul2_rn(c[QSV_COEF_M5], R0); u = __ffma2_rn(c[QSV_COEF_M4], I0, u); u = __ffma2_rn(c[QSV_COEF_M7], R1, u);
-    const float2 y1i = __ffma2_rn(c[QSV_COEF_M6], I1, u);
-    R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
-}
-__device__ __forceinline__ void dense2c_r0(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float2 *c) {
-    float2 t, u;
-    t = __fmul2_rn(c[QSV_COEF_NM3], I1); t = __ffma2_rn(c[QSV_COEF_M2], R1, t);
-    const float2 y0r = __ffma2_rn(c[QSV_COEF_M0], R0, t);
-    u = __fmul2_rn(c[QSV_COEF_M3], R1); u = __ffma2_rn(c[QSV_COEF_M2], I1, u);
-    const float2 y0i = __ffma2_rn(c[QSV_COEF_M0], I0, u);
-    t = __fmul2_rn(c[QSV_COEF_NM5], I0); t = __ffma2_rn(c[QSV_COEF_M4], R0, t); t = __ffma2_rn(c[QSV_COEF_NM7], I1, t);
-    const float2 y1r = __ffma2_rn(c[QSV_COEF_M6], R1, t);
-    u = __fmul2_rn(c[QSV_COEF_M5], R0); u = __ffma2_rn(c[QSV_COEF_M4], I0, u); u = __ffma2_rn(c[QSV_COEF_M7], R1, u);
-    const float2 y1i = __ffma2_rn(c[QSV_COEF_M6], I1, u);
-    R0 = y0r; I0 = y0i; R1 = y1r; I1 = y1i;
-}
-
-// register-bit dense ops (uniform, uniform with m00 real, controlled) with shared-memory coefficient pairs
-template <int NV, int RBIT, int VAR, int CMREG, uint32_t CMTHR>
-__device__ __forceinline__ void jit_reg_c(float2 (&R)[NV], float2 (&I)[NV], const float2 *c, uint32_t tb) {
-    constexpr int B = 1 << RBIT;
-    const bool tok = (CMTHR == 0u) || ((tb & CMTHR) == CMTHR);
-    if constexpr (VAR == QSV_V_UNI_DENSE) {
-#pragma unroll
-        for (int r = 0; r < NV; r++)
-            if (!(r & B)) dense2c(R[r], I[r], R[r | B], I[r | B], c);
-    } else if constexpr (VAR == QSV_V_UNI_DENSE_R0) {
-#pragma unroll
-        for (int r = 0; r < NV; r++)
-            if (!(r & B)) dense2c_r0(R[r], I[r], R[r | B], I[r | B], c);
-    } else {
-        static_assert(VAR == QSV_V_CTRL_DENSE, "shared-memory coefficients: dense variants only");
-        if (tok) {
-#pragma unroll
-            for (int r = 0; r < NV; r++)
-                if (!(r & B) && (r & CMREG) == CMREG) dense2c(R[r], I[r], R[r | B], I[r | B], c);
-        }
-    }
-}
-
 __device__ __forceinline__ void jit_mat(float (&m)[8], const float *src) {
 #pragma unroll
     for (int e = 0; e < 8; e++) m[e] = src[e];

@@ -59,22 +59,6 @@ typedef unsigned long long uint64_t;
 // chain are skipped. Used as a code path only; op records keep QSV_M_DENSE and set r00.
 #define QSV_M_DENSE_R0 5
 
-// positions of an op's 12 (c, c) coefficient pairs in the shared-memory coefficient table of specialised
-// kernels (m = the op's dense matrix as (re, im) x 4)
-#define QSV_COEF_M0 0
-#define QSV_COEF_M1 1
-#define QSV_COEF_NM1 2
-#define QSV_COEF_M2 3
-#define QSV_COEF_M3 4
-#define QSV_COEF_NM3 5
-#define QSV_COEF_M4 6
-#define QSV_COEF_M5 7
-#define QSV_COEF_NM5 8
-#define QSV_COEF_M6 9
-#define QSV_COEF_M7 10
-#define QSV_COEF_NM7 11
-#define QSV_COEF_PAIRS 12
-
 // op kinds
 #define QSV_K_UNI 0             // one matrix (M0) for every pair
 #define QSV_K_CTRL 1            // M0 = identity: pairs whose controls are all set get M1

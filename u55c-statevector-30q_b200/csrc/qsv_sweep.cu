@@ -32,7 +32,6 @@ struct InterpBody {
     using Amp = float2;
     static constexpr int kHalfBits = 1;
     static constexpr bool kSmemOps = true;
-    static constexpr bool kSmemCoef = false;
     template <int NV, int RB, int WB>
     static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *sops, int lane, int warp,
                                                 int bar) {

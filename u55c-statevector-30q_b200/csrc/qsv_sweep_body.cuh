@@ -71,14 +71,10 @@ __device__ __forceinline__ void tma_store(const CUtensorMap *map, const int32_t 
 // Dynamic shared memory a sweep kernel needs: S tile buffers, plus the op table when Body reads it there,
 // plus 1 KiB to align the buffers to 1024 bytes (the 128-byte swizzle pattern repeats every 1024 bytes of
 // shared-memory address, and the consumers' addressing assumes it starts at each buffer).
-// (Body::kSmemCoef: instead of the op table, each op's dense matrix as 12 (c, c) coefficient pairs,
-// QSV_COEF_* order, built by the CTA at start-up; a specialised kernel loads each pair with one shared-memory
-// load straight into the register pair its packed FP32x2 arithmetic reads.)
 template <int KW, int S, class Body, class SW = QsvSweep>
 __host__ __device__ constexpr size_t sweep_smem_bytes() {
     return ((size_t)S << KW) * sizeof(typename Body::Amp) +
-           (Body::kSmemOps ? sizeof(typename SW::op_type) * QSV_MAX_SWEEP_OPS : 0) +
-           (Body::kSmemCoef ? sizeof(float2) * QSV_COEF_PAIRS * QSV_MAX_SWEEP_OPS : 0) + QSV_SMEM_ALIGN;
+           (Body::kSmemOps ? sizeof(typename SW::op_type) * QSV_MAX_SWEEP_OPS : 0) + QSV_SMEM_ALIGN;
 }
 
 // The pipeline. Launch with G * (1 << (5 + WB)) + 32 threads and sweep_smem_bytes<KW, S, Body, SW>() bytes
@@ -119,18 +115,6 @@ __device__ __forceinline__ void sweep_pipeline(typename Body::Amp *__restrict__ 
         uint32_t *dst = reinterpret_cast<uint32_t *>(sops);
         const int words = P.nops * (int)(sizeof(Op) / 4);
         for (int i = tid; i < words; i += blockDim.x) dst[i] = src[i];
-    }
-    if constexpr (Body::kSmemCoef) {
-        // op o's pairs at [12 o, 12 o + 12): m[0], m[1], -m[1], m[2], m[3], -m[3], ... m[6], m[7], -m[7] of
-        // its dense matrix (M0 for uniform ops, M1 otherwise), as QSV_COEF_* index them
-        float2 *coef = reinterpret_cast<float2 *>(sops);
-        for (int i = tid; i < P.nops * QSV_COEF_PAIRS; i += blockDim.x) {
-            const int o = i / QSV_COEF_PAIRS, k = i % QSV_COEF_PAIRS;
-            const float *m = P.ops[o].kind == QSV_K_UNI ? P.ops[o].m0 : P.ops[o].m1;
-            const int src = 2 * (k / 3) + (k % 3 != 0);      // groups of 3: m[2g], m[2g+1], -m[2g+1]
-            const float v = (k % 3 == 2) ? -m[src] : m[src];
-            coef[i] = make_float2(v, v);
-        }
     }
     if (tid == 0) {
         for (int f = 0; f < NF; f++) mbar_init(&full[f], 1);

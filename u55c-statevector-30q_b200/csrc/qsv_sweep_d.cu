@@ -133,7 +133,6 @@ struct InterpBodyD {
     using Amp = double2;
     static constexpr int kHalfBits = 0;
     static constexpr bool kSmemOps = true;
-    static constexpr bool kSmemCoef = false;
     template <int NV, int RB, int WB>
     static __device__ __forceinline__ void tile(double2 *tile, const QsvSweepD &P, const QsvOpD *sops, int lane,
                                                 int warp, int bar) {
