@@ -166,7 +166,7 @@ for n, maker in ((14, lambda: gen.random_layer(14, 8, 13)), (20, lambda: gen.ran
     rng = np.random.default_rng(n)
     x = (rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)).astype(np.complex64)
     outs = []
-    for mode in ("off", "eager"):
+    for mode in ("off", "eager", "coarse"):
         engine.set_jit(mode)
         t = torch.from_numpy(x.copy()).cuda()
         for s in segs:
@@ -174,7 +174,7 @@ for n, maker in ((14, lambda: gen.random_layer(14, 8, 13)), (20, lambda: gen.ran
         torch.cuda.synchronize()
         outs.append(t.cpu().numpy())
     assert engine.device_status() == 0
-    assert np.array_equal(outs[0], outs[1]), n
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2]), n
     if n <= 20:
         ref = x.copy()
         for s in segs:
@@ -185,11 +185,13 @@ print("swizzled sweeps", swizzled)
 
 
 @pytest.mark.timeout(900)
-@pytest.mark.parametrize("env", [{"QSV_JIT_INTERLEAVE": "2"}, {"QSV_SWIZZLE": "0", "QSV_JIT_INTERLEAVE": "1"}])
+@pytest.mark.parametrize("env", [{"QSV_JIT_INTERLEAVE": "2"}, {"QSV_SWIZZLE": "0", "QSV_JIT_INTERLEAVE": "1"},
+                                 {"QSV_JIT_CM": "1"}, {"QSV_JIT_CM": "1", "QSV_JIT_GROUPS13": "1"}])
 def test_layout_switches_exact(torch, env, tmp_path):
-    """The non-default layout switches (read once per process, so run in a child process): phases of two
-    tiles interleaved in every multi-phase sweep; no swizzled layouts with interleaved tensor-map sweeps.
-    Specialised == interpreter == oracle, exactly."""
+    """The non-default code-generation switches (read once per process, so run in a child process): phases
+    of two tiles interleaved in every multi-phase sweep; no swizzled layouts with interleaved tensor-map
+    sweeps; coefficient-major dense ops, with two or one consumer groups. Specialised (exact and coarse
+    structures) == interpreter == oracle, exactly."""
     import os
     import subprocess
     import sys

@@ -92,6 +92,16 @@ int groups_for(const QsvSweep &sw, int wb) {
 // 0.5-2 % faster and the FP32-bound sweeps over qubits 0-12 5-15 % slower (their prefetch depth drops from
 // two tiles to one). QSV_JIT_INTERLEAVE=1: multi-phase tensor-map sweeps of one consumer group; =2: every
 // multi-phase sweep of one consumer group.
+// Whether uncontrolled dense ops on register bits use the coefficient-major form (jit_reg_cm). Tuning
+// switch QSV_JIT_CM=1; off by default.
+bool coef_major() {
+    static const bool on = [] {
+        const char *e = std::getenv("QSV_JIT_CM");
+        return e && std::atoi(e) == 1;
+    }();
+    return on;
+}
+
 int interleave_for(const QsvSweep &sw, int groups) {
     static const int mode = [] {
         const char *e = std::getenv("QSV_JIT_INTERLEAVE");
@@ -259,6 +269,10 @@ std::string gen_source(const QsvSweep &sw, int rb, int wb) {
             else if (op.slot < QSV_SLOT_LANE0 && op.variant == QSV_V_MUX)
                 s << "            jit_reg_mux<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << mux << ">(R, I, P.ops[" << o
                   << "], tb);\n";
+            else if (op.slot < QSV_SLOT_LANE0 && coef_major() &&
+                     (var == QSV_V_UNI_DENSE || var == QSV_V_UNI_DENSE_R0))
+                s << "            jit_reg_cm<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ">(R, I, P.ops[" << o
+                  << "]);\n";
             else if (op.slot < QSV_SLOT_LANE0)
                 s << "            jit_reg<NV, " << (op.slot - QSV_SLOT_REG0) << ", " << var << ", " << ctl
                   << ">(R, I, P.ops[" << o << "], tb);\n";
@@ -312,6 +326,7 @@ bool nvrtc_compile(const std::string &src, std::vector<char> &cubin, std::string
     nvrtcGetProgramLogSize(prog, &ls);
     log.assign(ls, '\0');
     if (ls) nvrtcGetProgramLog(prog, &log[0]);
+    while (!log.empty() && log.back() == '\0') log.pop_back();   // the size counts the terminator
     bool ok = r == NVRTC_SUCCESS;
     if (ok) {
         size_t n = 0;
@@ -353,7 +368,8 @@ void worker() {
         e->state = ok ? kReady : kFailed;
         if (ok) j.compiled++;
         else j.failed++;
-        if (!ok || std::getenv("QSV_JIT_PTXAS_VERBOSE")) j.last_log = log;
+        if (!ok) j.last_log = log;
+        else if (std::getenv("QSV_JIT_PTXAS_VERBOSE") && j.last_log.size() < (1u << 20)) j.last_log += log;  // all reports
         j.compile_ms += ms;
         j.busy--;
         j.done.notify_all();

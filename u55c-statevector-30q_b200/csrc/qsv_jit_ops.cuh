@@ -62,6 +62,100 @@ __device__ __forceinline__ void jit_store(float2 *tile, uint32_t tb, const float
     }
 }
 
+// Dense op on register bit RBIT, coefficient-major: every (c, c) pair is built once and applied to all 2^RB / 2
+// register pairs before the next one, so at most one pair is live at a time; each output keeps dense2's chain
+// (qsv_ops.cuh) term for term, so values are identical. Holds four partial sums per register pair (needs the
+// register budget of one consumer group). R0: m00 is real (its two imaginary terms, exact zeros, skipped).
+template <int NV, int RBIT, bool R0>
+__device__ __forceinline__ void jit_dense_cm(float2 (&R)[NV], float2 (&I)[NV], const float *m) {
+    constexpr int B = 1 << RBIT;
+    constexpr int NP = NV / 2;
+    float2 t0r[NP], t0i[NP], t1r[NP], t1i[NP];
+    auto lo = [](int p) { return (p & (B - 1)) | ((p & ~(B - 1)) << 1); };   // p-th register with bit RBIT clear
+    {
+        const float2 c = f2(-m[3]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t0r[p] = __fmul2_rn(c, I[lo(p) | B]);
+    }
+    {
+        const float2 c = f2(m[3]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t0i[p] = __fmul2_rn(c, R[lo(p) | B]);
+    }
+    {
+        const float2 c = f2(-m[5]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t1r[p] = __fmul2_rn(c, I[lo(p)]);
+    }
+    {
+        const float2 c = f2(m[5]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t1i[p] = __fmul2_rn(c, R[lo(p)]);
+    }
+    {
+        const float2 c = f2(m[2]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            t0r[p] = __ffma2_rn(c, R[lo(p) | B], t0r[p]);
+            t0i[p] = __ffma2_rn(c, I[lo(p) | B], t0i[p]);
+        }
+    }
+    {
+        const float2 c = f2(m[4]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            t1r[p] = __ffma2_rn(c, R[lo(p)], t1r[p]);
+            t1i[p] = __ffma2_rn(c, I[lo(p)], t1i[p]);
+        }
+    }
+    if constexpr (!R0) {
+        {
+            const float2 c = f2(-m[1]);
+#pragma unroll
+            for (int p = 0; p < NP; p++) t0r[p] = __ffma2_rn(c, I[lo(p)], t0r[p]);
+        }
+        {
+            const float2 c = f2(m[1]);
+#pragma unroll
+            for (int p = 0; p < NP; p++) t0i[p] = __ffma2_rn(c, R[lo(p)], t0i[p]);
+        }
+    }
+    {
+        const float2 c = f2(-m[7]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t1r[p] = __ffma2_rn(c, I[lo(p) | B], t1r[p]);
+    }
+    {
+        const float2 c = f2(m[7]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) t1i[p] = __ffma2_rn(c, R[lo(p) | B], t1i[p]);
+    }
+    {
+        const float2 c = f2(m[0]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            R[lo(p)] = __ffma2_rn(c, R[lo(p)], t0r[p]);
+            I[lo(p)] = __ffma2_rn(c, I[lo(p)], t0i[p]);
+        }
+    }
+    {
+        const float2 c = f2(m[6]);
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+            R[lo(p) | B] = __ffma2_rn(c, R[lo(p) | B], t1r[p]);
+            I[lo(p) | B] = __ffma2_rn(c, I[lo(p) | B], t1i[p]);
+        }
+    }
+}
+
+template <int NV, int RBIT, int VAR>
+__device__ __forceinline__ void jit_reg_cm(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op) {
+    float m[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) m[e] = op.m0[e];
+    jit_dense_cm<NV, RBIT, VAR == QSV_V_UNI_DENSE_R0>(R, I, m);
+}
+
 __device__ __forceinline__ void jit_mat(float (&m)[8], const float *src) {
 #pragma unroll
     for (int e = 0; e < 8; e++) m[e] = src[e];
