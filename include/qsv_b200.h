@@ -165,6 +165,13 @@ QSV_API int qsv_set_lo_merge(int lo);
  * per thread with 8 consumer warps (default) or 3 with 16. Values are identical either way. */
 QSV_API int qsv_set_layout13(int rb);
 
+/* Interpreter kernel for sweeps without a specialised kernel (no reference counterpart): 1 = streaming:
+ * the tile stays in shared memory and each group of consecutive ops touching at most three target qubits
+ * (plus ops on the lowest tile bit and diagonal ops anywhere) is one pass over it, 16 amplitudes per thread
+ * at a time; 0 = phase layouts (default): a thread keeps 32 amplitudes in registers per phase and exchanges
+ * lane bits with warp shuffles. Values are identical either way. Returns the previous mode; process-wide. */
+QSV_API int qsv_set_interp(int mode);
+
 /* Tuning knob (no reference counterpart): how many op targets a phase may place on lane bits (warp
  * shuffles) instead of starting a new phase, 0..2 (default 1). Values are identical either way. */
 QSV_API int qsv_set_phase_lanes(int k);

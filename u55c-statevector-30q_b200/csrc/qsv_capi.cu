@@ -13,6 +13,7 @@
 
 namespace qsv {
 cudaError_t launch_sweep(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream);
+int set_interp(int mode);
 cudaError_t launch_sweep_c128(double2 *state, const QsvSweepD &sw, int nsm, cudaStream_t stream);
 cudaError_t launch_remap(const void *src, void *dst, int n, const int32_t *perm, int dtype, int nsm,
                          cudaStream_t stream);
@@ -98,6 +99,12 @@ int qsv_set_lo_merge(int lo) {
 int qsv_set_layout13(int rb) {
     if (qsv::set_rb13(rb)) return fail(QSV_ERR_INVALID_ARG, "13-qubit layout takes 3 or 4 register bits");
     return QSV_OK;
+}
+
+int qsv_set_interp(int mode) {
+    const int prev = qsv::set_interp(mode);
+    if (prev < 0) return fail(QSV_ERR_INVALID_ARG, "interpreter mode must be 0 (phase layouts) or 1 (streaming)");
+    return prev;
 }
 
 int qsv_set_phase_lanes(int k) {

@@ -62,6 +62,49 @@ __device__ __forceinline__ void cmul2(float2 &R, float2 &I, float ar, float ai) 
     const float2 yi = __ffma2_rn(f2(ar), I, __fmul2_rn(f2(ai), R));
     R = yr; I = yi;
 }
+
+// The same chains as dense2 / dense2_r0 / cmul2, issued with every partial sum first and the final
+// multiply-adds last: each final is the last use of the input it replaces, so it can be written over that
+// input's register (code that dispatches ops at run time then keeps the amplitudes in place).
+__device__ __forceinline__ void dense2_ip(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float *m) {
+    float2 t0 = __fmul2_rn(f2(-m[3]), I1), u0 = __fmul2_rn(f2(m[3]), R1);
+    float2 t1 = __fmul2_rn(f2(-m[5]), I0), u1 = __fmul2_rn(f2(m[5]), R0);
+    t0 = __ffma2_rn(f2(m[2]), R1, t0); u0 = __ffma2_rn(f2(m[2]), I1, u0);
+    t1 = __ffma2_rn(f2(m[4]), R0, t1); u1 = __ffma2_rn(f2(m[4]), I0, u1);
+    t0 = __ffma2_rn(f2(-m[1]), I0, t0); u0 = __ffma2_rn(f2(m[1]), R0, u0);
+    t1 = __ffma2_rn(f2(-m[7]), I1, t1); u1 = __ffma2_rn(f2(m[7]), R1, u1);
+    R0 = __ffma2_rn(f2(m[0]), R0, t0); I0 = __ffma2_rn(f2(m[0]), I0, u0);
+    R1 = __ffma2_rn(f2(m[6]), R1, t1); I1 = __ffma2_rn(f2(m[6]), I1, u1);
+}
+__device__ __forceinline__ void dense2_r0_ip(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float *m) {
+    float2 t0 = __fmul2_rn(f2(-m[3]), I1), u0 = __fmul2_rn(f2(m[3]), R1);
+    float2 t1 = __fmul2_rn(f2(-m[5]), I0), u1 = __fmul2_rn(f2(m[5]), R0);
+    t0 = __ffma2_rn(f2(m[2]), R1, t0); u0 = __ffma2_rn(f2(m[2]), I1, u0);
+    t1 = __ffma2_rn(f2(m[4]), R0, t1); u1 = __ffma2_rn(f2(m[4]), I0, u1);
+    t1 = __ffma2_rn(f2(-m[7]), I1, t1); u1 = __ffma2_rn(f2(m[7]), R1, u1);
+    R0 = __ffma2_rn(f2(m[0]), R0, t0); I0 = __ffma2_rn(f2(m[0]), I0, u0);
+    R1 = __ffma2_rn(f2(m[6]), R1, t1); I1 = __ffma2_rn(f2(m[6]), I1, u1);
+}
+__device__ __forceinline__ void cmul2_ip(float2 &R, float2 &I, float ar, float ai) {
+    const float2 p = __fmul2_rn(f2(-ai), I), q = __fmul2_rn(f2(ai), R);
+    R = __ffma2_rn(f2(ar), R, p);
+    I = __ffma2_rn(f2(ar), I, q);
+}
+template <bool IP>
+__device__ __forceinline__ void dense2_t(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float *m) {
+    if constexpr (IP) dense2_ip(R0, I0, R1, I1, m);
+    else dense2(R0, I0, R1, I1, m);
+}
+template <bool IP>
+__device__ __forceinline__ void dense2_r0_t(float2 &R0, float2 &I0, float2 &R1, float2 &I1, const float *m) {
+    if constexpr (IP) dense2_r0_ip(R0, I0, R1, I1, m);
+    else dense2_r0(R0, I0, R1, I1, m);
+}
+template <bool IP>
+__device__ __forceinline__ void cmul2_t(float2 &R, float2 &I, float ar, float ai) {
+    if constexpr (IP) cmul2_ip(R, I, ar, ai);
+    else cmul2(R, I, ar, ai);
+}
 __device__ __forceinline__ void swap2(float2 &a, float2 &b) {
     const float2 t = a; a = b; b = t;
 }
@@ -69,8 +112,8 @@ __device__ __forceinline__ void swap2(float2 &a, float2 &b) {
 // ---------------------------------------------------------------- ops by target slot
 // Register-bit target RBIT: pairs (slot r, slot r | 2^RBIT); each float2 carries two pairs (tile bit 0 =
 // 0 in .x, 1 in .y). One tight unrolled loop per code variant (selected on the host).
-template <int NV, int RBIT>
-__device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, const float *m0,
+template <int NV, int RBIT, bool IP = false, class O = QsvOp>
+__device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
                                        const float *m1, bool thread_ok) {
     const int cm_reg = op.cm_reg;
 #define QSV_FOR_PAIRS for (int r = 0; r < NV; r++) if (!(r & (1 << RBIT)))
@@ -79,15 +122,15 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
         case QSV_V_UNI_DENSE:
             if (op.r00) {
 #pragma unroll
-                QSV_FOR_PAIRS dense2_r0(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+                QSV_FOR_PAIRS dense2_r0_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
             } else {
 #pragma unroll
-                QSV_FOR_PAIRS dense2(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+                QSV_FOR_PAIRS dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
             }
             break;
         case QSV_V_UNI_DIAG:
 #pragma unroll
-            QSV_FOR_PAIRS { cmul2(R[r], I[r], m0[0], m0[1]); cmul2(R[QSV_P1], I[QSV_P1], m0[6], m0[7]); }
+            QSV_FOR_PAIRS { cmul2_t<IP>(R[r], I[r], m0[0], m0[1]); cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m0[6], m0[7]); }
             break;
         case QSV_V_UNI_SWAP:
 #pragma unroll
@@ -95,11 +138,11 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
             break;
         case QSV_V_CTRL_DENSE:
 #pragma unroll
-            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) dense2(R[r], I[r], R[QSV_P1], I[QSV_P1], m1);
+            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m1);
             break;
         case QSV_V_CTRL_DIAG1:
 #pragma unroll
-            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) cmul2(R[QSV_P1], I[QSV_P1], m1[6], m1[7]);
+            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m1[6], m1[7]);
             break;
         case QSV_V_CTRL_SWAP:
 #pragma unroll
@@ -113,7 +156,7 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
                 float c[8];
 #pragma unroll
                 for (int e = 0; e < 8; e++) c[e] = s ? m1[e] : id[e];
-                dense2(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
+                dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
             }
             break;
         }
@@ -121,7 +164,7 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
 #pragma unroll
             QSV_FOR_PAIRS {
                 const bool s = thread_ok && (r & cm_reg) == cm_reg;
-                cmul2(R[QSV_P1], I[QSV_P1], s ? m1[6] : 1.f, s ? m1[7] : 0.f);
+                cmul2_t<IP>(R[QSV_P1], I[QSV_P1], s ? m1[6] : 1.f, s ? m1[7] : 0.f);
             }
             break;
         case QSV_V_CTRL_SWAP_SEL:
@@ -152,8 +195,8 @@ __device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const Q
 }
 
 // tile-bit-0 target: the pair is the two halves of one slot (scalar arithmetic, any variant)
-template <int NV>
-__device__ __forceinline__ void comp_op(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, const float *m0,
+template <int NV, class O = QsvOp>
+__device__ __forceinline__ void comp_op(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
                                      const float *m1, bool thread_ok) {
     const int cm_reg = op.cm_reg;
     const bool uni = op.kind == QSV_K_UNI, ctrl = op.kind == QSV_K_CTRL;
@@ -278,8 +321,8 @@ __device__ __forceinline__ void comp_loop(float2 (&R)[NV], float2 (&I)[NV], cons
     }
 }
 
-template <int NV>
-__device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], const QsvOp &op, const float *m0,
+template <int NV, class O = QsvOp>
+__device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
                                              const float *m1, bool tok) {
     const int cm_reg = op.cm_reg;
     if (op.kind == QSV_K_UNI) {
@@ -304,7 +347,7 @@ __device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], c
             default: break;
         }
     }
-    comp_op<NV>(R, I, op, m0, m1, tok);
+    comp_op<NV, O>(R, I, op, m0, m1, tok);
 }
 
 template <int NV>

@@ -84,11 +84,13 @@ typedef unsigned long long uint64_t;
 #define QSV_SLOT_COMP 0         // tile bit 0 (inside a float4)
 #define QSV_SLOT_REG0 1         // 1 + r: register bit r
 #define QSV_SLOT_LANE0 8        // 8 + l: lane bit l (warp shuffle)
+#define QSV_SLOT_BASE 7         // streaming interpreter: diagonal op on a tile bit of the item base
 
-struct QsvOp {
+// 96 bytes, 16-byte aligned: the matrices are four 16-byte vectors and every field a kernel reads is in
+// the 16 bytes at offset 64 (one vector load per op in the streaming interpreter).
+struct alignas(16) QsvOp {
     float m0[8];                // M0 = m00 m01 m10 m11 as (re, im)
     float m1[8];                // M1
-    uint32_t cmask;             // control mask over tile bits (0 = no controls)
     uint32_t cm_thr;            // the part of cmask on lane / warp tile bits (tested on the thread base)
     uint8_t cm_reg;             // the part of cmask on register bits, as a mask over the register index
     uint8_t cm_c;               // 1 if tile bit 0 is a control
@@ -100,6 +102,7 @@ struct QsvOp {
     uint8_t variant;            // QSV_V_*
     uint8_t r00;                // 1: M0 is dense with m00 real (QSV_M_DENSE_R0 path)
     uint8_t pad[2];
+    uint32_t cmask;             // control mask over tile bits (0 = no controls)
 };
 
 // complex128 op: the same fields with FP64 matrices. In the complex128 layout tile bits 0-2 are lane bits
@@ -143,6 +146,17 @@ struct QsvPhaseX {
     int32_t op_begin, op_end;
 };
 
+// Streaming interpreter (qsv_sweep.cu): a group of consecutive ops that runs as one shared-memory round
+// trip of the tile. A thread takes items of 8 float4 = 16 amplitudes, tile bits {0, q[0], q[1], q[2]}; the
+// group's ops target tile bit 0 or an item bit (register index bits 0-2 of the item), or are diagonal on
+// another tile bit (QSV_SLOT_BASE: the factor depends on a bit of the item's base).
+#define QSV_MAX_GROUPS 40       // every group but the last holds ops on three distinct target bits
+struct QsvGroup {
+    uint8_t q[3];               // item bits: distinct, in [1, kw)
+    uint8_t op_begin, op_end;
+    uint8_t pad[3];
+};
+
 template <class OpT>
 struct QsvSweepT {
     typedef OpT op_type;
@@ -166,6 +180,8 @@ struct QsvSweepT {
     int32_t skip_load;          // fault injection for tests: 1 = block 0 never loads its first tile (0: off)
     QsvPhase phases[QSV_MAX_PHASES];
     OpT ops[QSV_MAX_SWEEP_OPS];
+    int32_t ngroups;            // streaming plan (plan_stream; 0 until planned)
+    QsvGroup groups[QSV_MAX_GROUPS];
 };
 typedef QsvSweepT<QsvOp> QsvSweep;      // complex64 state, fp32 matrices
 typedef QsvSweepT<QsvOpD> QsvSweepD;    // complex128 state, fp64 matrices

@@ -529,6 +529,59 @@ template int build_sweeps<QsvOp>(const std::vector<PhysPass> &, int, int, int, s
 template int build_sweeps<QsvOpD>(const std::vector<PhysPass> &, int, int, int, std::vector<QsvSweepD> &,
                                   std::string &);
 
+// Groups for the streaming interpreter, greedy in op order: a group takes ops while their targets (tile
+// bits >= 1, except diagonal ops, which act element by element and so run on any tile bit of the item)
+// span at most three distinct tile bits; the fourth distinct target starts the next group. A group with
+// fewer than three such targets takes the highest free tile bits as item bits (their 16-byte chunks are
+// spread over all shared-memory banks). Every group but the last holds three ops on distinct targets, so a
+// sweep of at most QSV_MAX_SWEEP_OPS ops needs at most QSV_MAX_SWEEP_OPS / 3 + 1 groups.
+int plan_stream(QsvSweep &sw, std::string &err) {
+    static_assert(QSV_MAX_GROUPS >= QSV_MAX_SWEEP_OPS / 3 + 1, "group table too small");
+    const int kw = sw.kw, nops = sw.nops;
+    auto elementwise = [](const QsvOp &o) {
+        return o.variant == QSV_V_SKIP || o.variant == QSV_V_UNI_DIAG || o.variant == QSV_V_CTRL_DIAG1 ||
+               o.variant == QSV_V_CTRL_DIAG1_SEL;
+    };
+    int ng = 0;
+    for (int i = 0; i < nops;) {
+        int S[3] = {-1, -1, -1}, ns = 0, j = i;
+        auto has = [&](int t) { return t == S[0] || t == S[1] || t == S[2]; };
+        for (; j < nops; j++) {
+            const QsvOp &o = sw.ops[j];
+            if (o.tbit == 0 || elementwise(o) || has(o.tbit)) continue;
+            if (ns == 3) break;
+            S[ns++] = o.tbit;
+        }
+        for (int t = kw - 1; ns < 3 && t >= 1; t--)
+            if (!has(t)) S[ns++] = t;
+        if (ng == QSV_MAX_GROUPS || ns < 3) { err = "internal: streaming plan does not fit"; return QSV_ERR_UNSUPPORTED; }
+        QsvGroup &g = sw.groups[ng++];
+        std::memset(&g, 0, sizeof(g));
+        uint32_t item = 1u;
+        for (int k = 0; k < 3; k++) {
+            g.q[k] = (uint8_t)S[k];
+            item |= 1u << S[k];
+        }
+        g.op_begin = (uint8_t)i;
+        g.op_end = (uint8_t)j;
+        for (int o = i; o < j; o++) {
+            QsvOp &op = sw.ops[o];
+            const int t = op.tbit;
+            op.slot = QSV_SLOT_BASE;
+            if (t == 0) op.slot = QSV_SLOT_COMP;
+            op.cm_reg = 0;
+            for (int k = 0; k < 3; k++) {
+                if (t == S[k]) op.slot = (uint8_t)(QSV_SLOT_REG0 + k);
+                op.cm_reg |= (uint8_t)(((op.cmask >> S[k]) & 1u) << k);
+            }
+            op.cm_thr = op.cmask & ~item;
+        }
+        i = j;
+    }
+    sw.ngroups = ng;
+    return QSV_OK;
+}
+
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
     std::vector<int32_t> w;
     w.push_back((int32_t)sw.size());

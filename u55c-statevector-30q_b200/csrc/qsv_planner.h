@@ -51,6 +51,10 @@ int build_sweeps(const std::vector<PhysPass> &passes, int n, int kw, int lo_merg
 // in order, with its phases.
 int plan_whole_state(const std::vector<PhysPass> &passes, int n, std::vector<QsvOp> &ops_out,
                      std::vector<QsvPhaseX> &phases_out, std::string &err);
+// Re-plan a complex64 sweep for the streaming interpreter: groups of consecutive ops with at most three
+// distinct target tile bits >= 1 (ops on tile bit 0 and diagonal ops on other bits join any group), and
+// each op's slot / control split for its group's item layout. Replaces the phase fields of the ops.
+int plan_stream(QsvSweep &sw, std::string &err);
 // Flatten a plan into int32 words (layout documented in qsv_b200.h / the planner tests).
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap);
 

@@ -67,6 +67,7 @@ def load(path=LIB_PATH):
         "qsv_batch_upload": ([P, P, SZ, P], I32),
         "qsv_batch_launch": ([P, P, SZ, P], I32),
         "qsv_set_phase_lanes": ([ctypes.c_int], I32),
+        "qsv_set_interp": ([ctypes.c_int], I32),
         "qsv_set_jit": ([ctypes.c_int], I32),
         "qsv_set_wait_limit_us": ([ctypes.c_uint], I32),
         "qsv_inject_skip_load": ([ctypes.c_int], I32),
@@ -93,7 +94,7 @@ def exported_symbols():
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
             "qsv_sample_f64",
             "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
-            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_wait_limit_us",
+            "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_interp", "qsv_set_wait_limit_us",
             "qsv_inject_skip_load", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
             "qsv_jit_wait", "qsv_jit_info", "qsv_hbm_copy"]
@@ -329,6 +330,19 @@ def set_layout13(rb):
 
 def set_phase_lanes(k):
     _check(load().qsv_set_phase_lanes(int(k)))
+
+
+INTERP_MODES = {"phase": 0, "stream": 1}
+
+
+def set_interp(mode):
+    """Interpreter kernel for sweeps without a specialised kernel: "phase" (phase layouts in registers) or
+    "stream" (the tile stays in shared memory; groups of ops touching at most three target qubits run as
+    one pass over it). Values are identical. Returns the previous mode's name."""
+    rc = load().qsv_set_interp(INTERP_MODES[mode] if isinstance(mode, str) else int(mode))
+    if rc < 0:
+        _check(rc)
+    return {v: k for k, v in INTERP_MODES.items()}[rc]
 
 
 def hbm_copy(dst, src, stream=None):
