@@ -505,6 +505,8 @@ def main():
     ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off", "coarse"],
                     help="specialised sweep kernels (compiled before the warm-up unless off; coarse: kernels of "
                          "coarse sweep structures only)")
+    ap.add_argument("--interp", default=None, choices=["phase", "stream"],
+                    help="interpreter kernel for sweeps without a specialised kernel (default: the library's)")
     ap.add_argument("--family", default="random_layer", choices=["random_layer", "rqc", "vqe", "qft"],
                     help="rl30 workload circuit: the headline random-layer circuit (default) or, for profiles, "
                          "a reference family")
@@ -577,6 +579,8 @@ def main():
     engine.load()
     sweeps = sum(len(engine.plan_segment(s, a.n)) for s in segs)
     eng_info = {"sweeps": sweeps}
+    if a.interp:
+        engine.set_interp(a.interp)
     engine.set_jit(a.jit)
     if a.jit != "off":
         t0 = time.perf_counter()
