@@ -186,11 +186,12 @@ print("swizzled sweeps", swizzled)
 
 @pytest.mark.timeout(900)
 @pytest.mark.parametrize("env", [{"QSV_JIT_INTERLEAVE": "2"}, {"QSV_SWIZZLE": "0", "QSV_JIT_INTERLEAVE": "1"},
-                                 {"QSV_JIT_CM": "1"}, {"QSV_JIT_CM": "1", "QSV_JIT_GROUPS13": "1"}])
+                                 {"QSV_JIT_CM": "1"}, {"QSV_JIT_CM": "1", "QSV_JIT_GROUPS13": "1"},
+                                 {"QSV_JIT_STREAM": "1"}])
 def test_layout_switches_exact(torch, env, tmp_path):
     """The non-default code-generation switches (read once per process, so run in a child process): phases
     of two tiles interleaved in every multi-phase sweep; no swizzled layouts with interleaved tensor-map
-    sweeps; coefficient-major dense ops, with two or one consumer groups. Specialised (exact and coarse
+    sweeps; coefficient-major dense ops, with two or one consumer groups; streaming-form kernels. Specialised (exact and coarse
     structures) == interpreter == oracle, exactly."""
     import os
     import subprocess

@@ -15,7 +15,7 @@ LIB = os.path.join(HERE, "libqsv_b200.so")
 SOURCES = ["qsv_capi.cu", "qsv_sweep.cu", "qsv_sweep_d.cu", "qsv_aux.cu", "qsv_batch.cu", "qsv_planner.cpp",
            "qsv_jit.cpp"]
 # device headers compiled into the library AND embedded in it for run-time (NVRTC) specialised kernels
-JIT_HEADERS = ["qsv_plan.h", "qsv_device.cuh", "qsv_ops.cuh", "qsv_sweep_body.cuh", "qsv_jit_ops.cuh"]
+JIT_HEADERS = ["qsv_plan.h", "qsv_device.cuh", "qsv_ops.cuh", "qsv_sweep_body.cuh", "qsv_jit_ops.cuh", "qsv_stream.cuh"]
 HEADERS = JIT_HEADERS + ["qsv_planner.h"]
 GEN = os.path.join(CSRC, "_gen", "qsv_jit_headers.inc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -148,6 +148,7 @@ struct Entry {
     std::string log;
     long long uses = 0;
     bool coarse = false;        // a coarse structure's kernel (coarse_of)
+    bool stream = false;        // a streaming-form kernel (gen_source_stream; op table in shared memory)
     double work = 0.0;          // amplitudes swept by this structure's launches
     CUfunction fn[kMaxDevices] = {nullptr};
     int per_sm[kMaxDevices] = {0};
@@ -223,6 +224,65 @@ std::string key_of(const QsvSweep &sw, int rb, int wb) {
         put(op.kind); put(op.cls0); put(op.cls1); put(op.cm_c); put(op.r00);
     }
     return k;
+}
+
+// Streaming form (QSV_JIT_STREAM=1; sw planned by plan_stream): a kernel per sequence of groups, each group
+// straight-line code for its ops' slots, variants, kinds, matrix classes and r00; item bits, control masks,
+// target bits and matrices are read at run time, so every sweep with the same sequence shares the kernel.
+bool stream_form() {
+    static const bool on = [] {
+        const char *e = std::getenv("QSV_JIT_STREAM");
+        return e && std::atoi(e) == 1;
+    }();
+    return on;
+}
+
+std::string stream_key_of(const QsvSweep &sw, int rb, int wb) {
+    std::string k;
+    auto put = [&](int v) { k.push_back((char)(v & 0xff)); };
+    put(sw.kw); put(rb); put(wb); put(sw.swz); put(sw.ngroups); put(sw.nops);
+    for (int g = 0; g < sw.ngroups; g++) { put(sw.groups[g].op_begin); put(sw.groups[g].op_end); }
+    for (int o = 0; o < sw.nops; o++) {
+        const QsvOp &op = sw.ops[o];
+        put(op.slot); put(op.variant); put(op.kind); put(op.cls0); put(op.cls1); put(op.r00);
+    }
+    return k;
+}
+
+std::string gen_source_stream(const QsvSweep &sw, int rb, int wb) {
+    const int nc = 1 << (5 + wb), nt = nc + 32, minb = sw.kw >= 13 ? 1 : 2;
+    std::ostringstream s;
+    s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_stream.cuh\"\n"
+      << "namespace qsv {\nnamespace dev {\nstruct JitBody {\n"
+      << "    using Amp = float2;\n"
+      << "    static constexpr int kHalfBits = 1;\n"
+      << "    static constexpr bool kSmemOps = true;\n"
+      << "    template <int NV, int RB, int WB>\n"
+      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *ops, int lane, int warp,\n"
+      << "                                                int bar) {\n"
+      << "        const int ctid = warp * 32 + lane;\n";
+    for (int g = 0; g < sw.ngroups; g++) {
+        const QsvGroup &G = sw.groups[g];
+        if (g > 0) s << "        named_bar_sync(bar, " << nc << ");\n";
+        s << "        stream_items<" << sw.kw << ", " << nc << ", " << (g > 0 ? "true" : "false") << ", "
+          << (g + 1 < sw.ngroups ? "true" : "false") << ">(tile, P.groups[" << g << "], ctid, "
+          << (sw.swz ? "true" : "false") << ", [&](float2 (&R)[8], float2 (&I)[8], uint32_t x) {\n";
+        for (int o = G.op_begin; o < G.op_end; o++) {
+            const QsvOp &op = sw.ops[o];
+            if (op.variant == QSV_V_SKIP) continue;
+            s << "            stream_op_fixed<true, " << (int)op.slot << ", " << (int)op.variant << ", " << (int)op.kind
+              << ", " << (int)op.cls0 << ", " << (int)op.cls1 << ", " << (int)op.r00 << ">(ops + " << o
+              << ", R, I, x);\n";
+        }
+        s << "        });\n";
+    }
+    s << "    }\n};\n}  // namespace dev\n}  // namespace qsv\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb << ")\n"
+      << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
+      << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
+      << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages
+      << ", 1, qsv::dev::JitBody, QsvSweep, 0>(state, P, &tmap, status);\n}\n";
+    return s.str();
 }
 
 // CUDA source of the kernel specialised to sw's structure
@@ -409,7 +469,7 @@ void warm_up_nvrtc() {
 // with j.mu held: queue e for compilation (starts the compile threads on first use)
 void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
     if (e->state != kNew) return;
-    e->src = gen_source(sw, e->rb, e->wb);
+    e->src = e->stream ? gen_source_stream(sw, e->rb, e->wb) : gen_source(sw, e->rb, e->wb);
     e->state = kQueued;
     j.queue.push_back(e);
     if (j.stopping) {
@@ -428,8 +488,9 @@ void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
     j.work.notify_one();
 }
 
-std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, bool coarse = false) {
-    const std::string key = (coarse ? "C" : "E") + key_of(sw, rb, wb);
+std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, bool coarse = false,
+                                   bool stream = false) {
+    const std::string key = stream ? "S" + stream_key_of(sw, rb, wb) : (coarse ? "C" : "E") + key_of(sw, rb, wb);
     auto it = j.map.find(key);
     if (it != j.map.end()) return it->second;
     if (j.map.size() >= kMaxEntries) {
@@ -444,8 +505,9 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, b
     e->kw = sw.kw;
     e->rb = rb;
     e->wb = wb;
-    e->groups = groups_for(sw, wb);
+    e->groups = stream ? 1 : groups_for(sw, wb);
     e->coarse = coarse;
+    e->stream = stream;
     j.map.emplace(key, e);
     return e;
 }
@@ -471,6 +533,15 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
     for (const QsvSweep &sw : sweeps) {
         int rb = 0, wb = 0;
         if (layout_for_kw(sw.kw, &rb, &wb)) continue;
+        if (stream_form()) {
+            QsvSweep s2 = sw;
+            std::string err;
+            if (plan_stream(s2, err) != QSV_OK) continue;
+            auto e = find_or_add(j, s2, rb, wb, false, true);
+            enqueue(j, e, s2);
+            mine.push_back(e);
+            continue;
+        }
         if (j.mode == 3) {
             const QsvSweep c = coarse_of(sw);
             auto e = find_or_add(j, c, rb, wb, true);
@@ -524,18 +595,27 @@ std::string jit_last_log() {
 
 // Launch sw with its specialised kernel if that kernel is ready (compiling it first in eager mode).
 // Returns 1 if launched, 0 if the caller should run the interpreter, -1 on a CUDA error (*err set).
-int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stream, cudaError_t *err) {
+int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t stream, cudaError_t *err) {
     Jit &j = J();
     int rb = 0, wb = 0;
-    if (layout_for_kw(sw.kw, &rb, &wb)) return 0;
+    if (layout_for_kw(sw_in.kw, &rb, &wb)) return 0;
+    // streaming form: the kernel runs the sweep re-planned into groups
+    thread_local QsvSweep s2;
+    const bool sf = stream_form();
+    if (sf) {
+        std::memcpy(&s2, &sw_in, sizeof(QsvSweep));
+        std::string perr;
+        if (plan_stream(s2, perr) != QSV_OK) return 0;
+    }
+    const QsvSweep &sw = sf ? s2 : sw_in;
     const Drv &d = drv();
     std::shared_ptr<Entry> e;
     {
         std::unique_lock<std::mutex> lk(j.mu);
         if (j.mode == 0 || !d.ok) { j.interp_launches++; return 0; }
         const double work = (double)sw.ntiles * (double)(1 << sw.kw);
-        if (j.mode != 3) {
-            e = find_or_add(j, sw, rb, wb);
+        if (j.mode != 3 || sf) {
+            e = find_or_add(j, sw, rb, wb, false, sf);
             e->uses++;
             e->work += work;
             if (e->state == kNew &&
@@ -543,7 +623,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
                 enqueue(j, e, sw);
             if (j.mode == 1) j.done.wait(lk, [&] { return e->state != kQueued; });
         }
-        if ((!e || e->state != kReady) && (j.mode == 2 || j.mode == 3)) {
+        if (!sf && (!e || e->state != kReady) && (j.mode == 2 || j.mode == 3)) {
             // the kernel of the sweep's coarse structure, shared with every sweep of that structure
             const QsvSweep c = coarse_of(sw);
             std::shared_ptr<Entry> ce = find_or_add(j, c, rb, wb, true);
@@ -562,7 +642,8 @@ int jit_try_launch(float2 *state, const QsvSweep &sw, int nsm, cudaStream_t stre
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
     const int NT = e->groups * (1 << (5 + wb)) + 32;
     // sweep_smem_bytes of the generated body: the tile buffers plus 1 KiB for their 1024-byte alignment
-    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN;
+    const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN +
+                        (e->stream ? sizeof(QsvOp) * QSV_MAX_SWEEP_OPS : 0);
     if (!e->fn[dev]) {
         // loading a module is not a stream operation: keep it out of stream captures
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;

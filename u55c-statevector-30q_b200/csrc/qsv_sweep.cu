@@ -22,6 +22,7 @@
 #include "qsv_device.cuh"
 #include "qsv_ops.cuh"
 #include "qsv_planner.h"
+#include "qsv_stream.cuh"
 #include "qsv_sweep_body.cuh"
 
 namespace qsv {
@@ -62,102 +63,6 @@ static_assert(sizeof(QsvOp) == 96 && offsetof(QsvOp, cm_thr) == 64 && offsetof(Q
                   offsetof(QsvOp, cls0) == 72 && offsetof(QsvOp, variant) == 76 && offsetof(QsvOp, m1) == 32,
               "op_hdr reads the op record's fields as one 16-byte vector at offset 64");
 
-// The fields of an op record a kernel reads, from one 16-byte shared-memory load.
-struct OpHdr {
-    uint32_t cm_thr, cm_reg, cm_c, kind, cls0, cls1, slot, tbit, variant, r00;
-};
-__device__ __forceinline__ OpHdr op_hdr(const QsvOp *op) {
-    const uint4 h = *reinterpret_cast<const uint4 *>(reinterpret_cast<const unsigned char *>(op) + 64);
-    OpHdr o;
-    o.cm_thr = h.x;
-    o.cm_reg = h.y & 0xffu; o.cm_c = (h.y >> 8) & 0xffu; o.kind = (h.y >> 16) & 0xffu;
-    o.cls0 = h.z & 0xffu; o.cls1 = (h.z >> 8) & 0xffu; o.slot = (h.z >> 16) & 0xffu; o.tbit = h.z >> 24;
-    o.variant = h.w & 0xffu; o.r00 = (h.w >> 8) & 0xffu;
-    return o;
-}
-
-// diagonal op whose target is a tile bit of the item base: every amplitude of the item has the same
-// target-bit value `one`
-template <int NV, bool IP>
-__device__ __forceinline__ void base_diag(float2 (&R)[NV], float2 (&I)[NV], const OpHdr &op, const float *m0,
-                                          const float *m1, bool tok, bool one) {
-    if (op.variant == QSV_V_UNI_DIAG) {
-        const float ar = one ? m0[6] : m0[0], ai = one ? m0[7] : m0[1];
-#pragma unroll
-        for (int r = 0; r < NV; r++) cmul2_t<IP>(R[r], I[r], ar, ai);
-        return;
-    }
-    // QSV_V_CTRL_DIAG1(_SEL): amplitudes with the target bit and every control set get m11
-    if (!(one && tok)) return;
-    const int cm_reg = (int)op.cm_reg;
-#pragma unroll
-    for (int r = 0; r < NV; r++)
-        if ((r & cm_reg) == cm_reg) cmul2_t<IP>(R[r], I[r], m1[6], m1[7]);
-}
-
-template <bool IP>
-__device__ __forceinline__ void stream_op(const QsvOp *op, float2 (&R)[8], float2 (&I)[8], uint32_t base) {
-    const OpHdr h = op_hdr(op);
-    if (h.variant == QSV_V_SKIP) return;
-    float m0[8], m1[8];
-    const float4 *mv = reinterpret_cast<const float4 *>(op);
-#pragma unroll
-    for (int v = 0; v < 2; v++) {
-        const float4 a = mv[v], c = mv[2 + v];
-        m0[4 * v] = a.x; m0[4 * v + 1] = a.y; m0[4 * v + 2] = a.z; m0[4 * v + 3] = a.w;
-        m1[4 * v] = c.x; m1[4 * v + 1] = c.y; m1[4 * v + 2] = c.z; m1[4 * v + 3] = c.w;
-    }
-    const bool tok = (base & h.cm_thr) == h.cm_thr;
-    switch (h.slot) {
-        case QSV_SLOT_COMP: comp_op_fast<8>(R, I, h, m0, m1, tok); break;
-        case QSV_SLOT_REG0: reg_op<8, 0, IP>(R, I, h, m0, m1, tok); break;
-        case QSV_SLOT_REG0 + 1: reg_op<8, 1, IP>(R, I, h, m0, m1, tok); break;
-        case QSV_SLOT_REG0 + 2: reg_op<8, 2, IP>(R, I, h, m0, m1, tok); break;
-        case QSV_SLOT_BASE: base_diag<8, IP>(R, I, h, m0, m1, tok, (base >> h.tbit) & 1u); break;
-        default: break;
-    }
-}
-
-// insert a zero bit at position q (bits q and above move up by one)
-__device__ __forceinline__ uint32_t insert0(uint32_t x, uint32_t q) {
-    return ((x >> q) << (q + 1)) | (x & ((1u << q) - 1u));
-}
-
-// One group over the whole tile. SIN / SOUT: the tile holds the in-tile order (re0, re1, im0, im1) per
-// float4 on entry / exit, instead of the state's interleaved order (first group in, last group out).
-template <int KW, int NCG, bool SIN, bool SOUT, bool IP>
-__device__ __forceinline__ void stream_group(float2 *tile, const QsvOp *sops, const QsvGroup &g, int ctid, bool swz) {
-    const uint32_t q[3] = {g.q[0], g.q[1], g.q[2]};
-    uint32_t soff[8];
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-        const uint32_t o = ((r & 1) ? 1u << q[0] : 0u) | ((r & 2) ? 1u << q[1] : 0u) | ((r & 4) ? 1u << q[2] : 0u);
-        soff[r] = swz ? swz128(o) : o;
-    }
-    // the item bits in ascending order, for the zero insertions
-    uint32_t s0 = q[0], s1 = q[1], s2 = q[2], t;
-    if (s0 > s1) { t = s0; s0 = s1; s1 = t; }
-    if (s1 > s2) { t = s1; s1 = s2; s2 = t; }
-    if (s0 > s1) { t = s0; s0 = s1; s1 = t; }
-    const int ob = g.op_begin, oe = g.op_end;
-    for (int it = ctid; it < (1 << (KW - 4)); it += NCG) {
-        const uint32_t x = insert0(insert0(insert0((uint32_t)it << 1, s0), s1), s2);
-        const uint32_t sx = swz ? swz128(x) : x;                          // swz128 is linear over XOR
-        float2 R[8], I[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) {
-            const float4 v = *reinterpret_cast<const float4 *>(tile + (sx ^ soff[r]));
-            R[r] = SIN ? make_float2(v.x, v.y) : make_float2(v.x, v.z);
-            I[r] = SIN ? make_float2(v.z, v.w) : make_float2(v.y, v.w);
-        }
-        for (int o = ob; o < oe; o++) stream_op<IP>(sops + o, R, I, x);
-#pragma unroll
-        for (int r = 0; r < 8; r++)
-            *reinterpret_cast<float4 *>(tile + (sx ^ soff[r])) =
-                SOUT ? make_float4(R[r].x, R[r].y, I[r].x, I[r].y) : make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
-    }
-}
-
 template <bool IP>
 struct StreamBody {
     using Amp = float2;
@@ -175,10 +80,14 @@ struct StreamBody {
             if (gi > 0) named_bar_sync(bar, NCG);
             const QsvGroup g = P.groups[gi];
             const bool sin = gi > 0, sout = gi + 1 < ng;
-            if (sin && sout) stream_group<KW, NCG, true, true, IP>(tile, sops, g, ctid, swz);
-            else if (sin) stream_group<KW, NCG, true, false, IP>(tile, sops, g, ctid, swz);
-            else if (sout) stream_group<KW, NCG, false, true, IP>(tile, sops, g, ctid, swz);
-            else stream_group<KW, NCG, false, false, IP>(tile, sops, g, ctid, swz);
+            const int ob = g.op_begin, oe = g.op_end;
+            auto ops = [&](float2 (&R)[8], float2 (&I)[8], uint32_t x) {
+                for (int o = ob; o < oe; o++) stream_op<IP>(sops + o, R, I, x);
+            };
+            if (sin && sout) stream_items<KW, NCG, true, true>(tile, g, ctid, swz, ops);
+            else if (sin) stream_items<KW, NCG, true, false>(tile, g, ctid, swz, ops);
+            else if (sout) stream_items<KW, NCG, false, true>(tile, g, ctid, swz, ops);
+            else stream_items<KW, NCG, false, false>(tile, g, ctid, swz, ops);
         }
     }
 };
