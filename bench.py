@@ -244,6 +244,15 @@ def batched_main(a):
             work_bytes += 16 << n
         else:
             work_bytes += sum(len(engine.plan_segment(seg, n)) for kind, seg in prog if kind == "segment") * (16 << n)
+    # the group-type library for the 13-qubit sweeps of the batch's larger circuits (one build before the
+    # timed work; the plain path below uses it too)
+    lib_info = None
+    if a.jit in ("auto", "library"):
+        t0 = time.perf_counter()
+        big = [(seg, n) for qc, (prog, fmap, n, npass) in zip(circs, progs) if n > batch.SMALL_MAX
+               for kind, seg in prog if kind == "segment"]
+        lib_info = {"types": engine.jit_prepare_library(big) if big else 0,
+                    "build_s": round(time.perf_counter() - t0, 2)}
     br = batch.BatchRunner(streams=8, autotune=True)
     plan = br.prepare(circs, programs=progs)
     br.capture(plan)
@@ -292,7 +301,7 @@ def batched_main(a):
                                      "note": "new batch from circuits: compile in a running worker pool + plan + one pass, vs "
                                              "compile and run one circuit at a time"},
                       "algorithmic_bytes": work_bytes, "hbm_floor_s": work_bytes / (_peaks()[0] * 1e9),
-                      "graph_launches": plan.launches, "host_compile_s": t_compile,
+                      "graph_launches": plan.launches, "host_compile_s": t_compile, "group_library": lib_info,
                       "specialised_kernels": engine.jit_info(), "clocks": clk.summary()}))
 
 
@@ -502,7 +511,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the complex128 (FP64) comparison runs")
-    ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off", "coarse"],
+    ap.add_argument("--jit", default="auto", choices=["auto", "eager", "off", "coarse", "library"],
                     help="specialised sweep kernels (compiled before the warm-up unless off; coarse: kernels of "
                          "coarse sweep structures only)")
     ap.add_argument("--interp", default=None, choices=["phase", "stream"],

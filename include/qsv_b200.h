@@ -187,23 +187,39 @@ QSV_API int qsv_set_phase_lanes(int k);
  * 2 = automatic (default): a structure is compiled in background threads once its launches have swept
  * 2^31 amplitudes in total (two sweeps of a 30-qubit state, 512 of a 22-qubit one; at most 64 compilations
  * wait at a time), and used from the first launch after its kernel is ready; until then the sweep runs its
- * coarse structure's kernel, compiled once the sweeps sharing it have swept 2^30 amplitudes, or the
- * interpreter; 3 = eager with coarse structures only. Switching to mode 0 drops waiting compilations and
- * waits for running ones. Returns the previous mode. Process-wide. */
+ * coarse structure's kernel, compiled once the sweeps sharing it have swept 2^30 amplitudes, or (13-qubit
+ * windows) the group-type library, or the interpreter; 3 = eager with coarse structures only; 4 = the
+ * group-type library only (qsv_jit_prepare builds it, blocking, to cover a segment's 13-qubit sweeps).
+ * The group-type library is one kernel holding straight-line code for up to 32 op sequences of one group
+ * of the streaming form (per op: slot among the group's three item bits, code variant, kind, matrix
+ * classes), the ones that have swept the most amplitudes, with item bits, control masks and matrices read
+ * at run time; it serves sweeps whose exact and coarse structures never repeat once 3/4 of their ops fall
+ * in its cases, and is rebuilt in the background after groups outside it have swept 2^31 amplitudes.
+ * Switching to mode 0 drops waiting compilations and waits for running ones. Returns the previous mode.
+ * Process-wide. */
 QSV_API int qsv_set_jit(int mode);
 
 /* Compile, in parallel and blocking, the specialised kernels of every sweep of a segment for an n-qubit
- * state (host work only; no device is touched): exact structures, or coarse ones in mode 3. Returns how
- * many of the segment's sweeps have a ready kernel, or a negative error code for a malformed segment. */
+ * state (host work only; no device is touched): exact structures, coarse ones in mode 3, a group-type
+ * library covering the segment's 13-qubit sweeps in mode 4. Returns how many of the segment's sweeps have a
+ * ready kernel, or a negative error code for a malformed segment. */
 QSV_API int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n);
+
+/* Build (blocking, host work only) the group-type library (qsv_set_jit) from the 13-qubit sweeps of count
+ * programs (segment i: segs[i], nwords[i] words, for an ns[i]-qubit state): their group types' swept
+ * amplitudes are recorded and the library takes the 32 most swept types seen so far. A batch or a service
+ * calls it once before its timed or latency-bound work. Returns the number of types in the library, or a
+ * negative error code (malformed segment; QSV_ERR_CUDA if the library does not compile). */
+QSV_API int qsv_jit_prepare_library(const int32_t *const *segs, const size_t *nwords, const int *ns, int count);
 
 /* Block until every queued background compilation has finished. */
 QSV_API int qsv_jit_wait(void);
 
-/* Counters of the specialised-kernel cache, written to out[0 .. min(cap, 10)): mode, structures seen
+/* Counters of the specialised-kernel cache, written to out[0 .. min(cap, 12)): mode, structures seen
  * (exact and coarse), kernels ready, compilations failed, sweeps launched specialised (exact or coarse),
  * sweeps launched interpreted, total compile milliseconds, compilations queued or running, sweeps launched
- * with a coarse structure's kernel, coarse structures seen. Returns 10. */
+ * with a coarse structure's kernel, coarse structures seen, sweeps launched with the group-type library,
+ * group types in the library in use. Returns 12. */
 QSV_API int qsv_jit_info(long long *out, int cap);
 
 #ifdef __cplusplus

@@ -92,3 +92,22 @@ def test_exit_with_compilations_in_flight():
     )
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.timeout(900)
+def test_group_type_library_compiles(lib):
+    """The group-type library (one kernel with a case per group type of the streaming form) compiles for the
+    types of a random-Toffoli circuit and a Grover circuit, keeps at most 32 of them, and is the library in
+    use afterwards (host work only)."""
+    progs = []
+    for n, maker in ((18, lambda: gen.random_layer_ccx(18, 8, 5)), (14, lambda: gen.grover(14, 2))):
+        prog, _, _ = q.compile_circuit(maker(), n, 12)
+        progs += [(seg, n) for kind, seg in prog if kind == "segment"]
+    old = engine.set_jit("library")
+    try:
+        types = engine.jit_prepare_library(progs)
+        info = engine.jit_info()
+    finally:
+        engine.set_jit(old)
+    assert 0 < types <= 32
+    assert info["lib_types"] == types and info["failed"] == 0

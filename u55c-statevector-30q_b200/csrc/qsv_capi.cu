@@ -36,6 +36,7 @@ cudaError_t launch_reduce_noalloc(const void *state, int n, int dtype, double *o
 size_t noalloc_reduce_capacity();
 int jit_set_mode(int mode);
 int jit_prepare(const std::vector<QsvSweep> &sweeps);
+int jit_prepare_library(const std::vector<QsvSweep> &sweeps);
 void jit_wait();
 int jit_info(long long *out, int cap);
 std::string jit_last_log();
@@ -182,7 +183,7 @@ int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int d
 
 int qsv_set_jit(int mode) {
     const int old = qsv::jit_set_mode(mode);
-    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "jit mode must be 0, 1, 2 or 3");
+    if (old < 0) return fail(QSV_ERR_INVALID_ARG, "jit mode must be 0, 1, 2, 3 or 4");
     return old;
 }
 
@@ -200,6 +201,27 @@ int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n) {
     const std::string log = qsv::jit_last_log();
     if (!log.empty()) t_err = log;
     return ready;
+}
+
+int qsv_jit_prepare_library(const int32_t *const *segs, const size_t *nwords, const int *ns, int count) {
+    if (count < 0 || (count > 0 && (!segs || !nwords || !ns))) return fail(QSV_ERR_INVALID_ARG, "null segment list");
+    std::vector<QsvSweep> all;
+    for (int i = 0; i < count; i++) {
+        const int n = ns[i];
+        if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+        std::vector<qsv::PhysPass> passes;
+        std::string err;
+        int rc = qsv::decode_segment(segs[i], nwords[i], n, passes, err);
+        if (rc) return fail(rc, err);
+        std::vector<QsvSweep> sweeps;
+        const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+        rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
+        if (rc) return fail(rc, err);
+        all.insert(all.end(), sweeps.begin(), sweeps.end());
+    }
+    const int types = qsv::jit_prepare_library(all);
+    if (types < 0) return fail(QSV_ERR_CUDA, "group-type library failed to compile: " + qsv::jit_last_log());
+    return types;
 }
 
 int qsv_jit_wait(void) {

@@ -32,6 +32,7 @@
 #include <nvrtc.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -154,6 +155,14 @@ struct Entry {
     int per_sm[kMaxDevices] = {0};
 };
 
+// a compiled (or compiling) group-type library: its cases in order
+struct Lib {
+    int rb = 0, wb = 0;
+    std::vector<std::string> types;
+    std::unordered_map<std::string, int> index;
+    std::shared_ptr<Entry> entry;
+};
+
 struct Jit {
     std::mutex mu;
     std::condition_variable work, done;
@@ -163,6 +172,11 @@ struct Jit {
     bool stopping = false;      // set at process exit: workers take no new work
     int mode = 2;
     long long jit_launches = 0, interp_launches = 0, coarse_launches = 0, compiled = 0, failed = 0;
+    // group-type library: amplitudes swept per group type, the library in use and the one being built
+    std::unordered_map<std::string, double> gweight;
+    std::shared_ptr<Lib> lib, lib_next;
+    double lib_uncovered = 0.0;
+    long long lib_launches = 0;
     double compile_ms = 0.0;
     std::string last_log;
 };
@@ -281,6 +295,77 @@ std::string gen_source_stream(const QsvSweep &sw, int rb, int wb) {
       << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
       << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
       << "    qsv::dev::sweep_pipeline<" << sw.kw << ", " << rb << ", " << wb << ", " << kStages
+      << ", 1, qsv::dev::JitBody, QsvSweep, 0>(state, P, &tmap, status);\n}\n";
+    return s.str();
+}
+
+// ---------------------------------------------------------------- group-type library
+// Sweeps whose exact and coarse structures never repeat (random gate choices, random Toffoli positions)
+// still repeat at the level of one group of the streaming form: the op sequence of a group (per op: slot
+// among the item bits, variant, kind, matrix classes, r00) recurs across sweeps and circuits. The library
+// is ONE kernel for 13-qubit windows with straight-line code for each of up to kLibMaxTypes group types and
+// a run-time-dispatch path for the others; it is rebuilt, in the background, from the types that have
+// swept the most amplitudes. Item bits, control masks and matrices are read at run time.
+constexpr int kLibMaxTypes = 32;        // front-end compile time grows faster than linearly with the cases
+                                        // (10 / 20 / 40 / 86 cases: 4 / 7 / 17 / ~80 s); the 16 / 64 most
+                                        // swept group types cover 87 / 94 % of the groups of a mixed batch
+constexpr double kLibThreshold = 2147483648.0;   // amplitudes swept by groups outside the library before a rebuild
+constexpr size_t kLibMaxSeen = 1u << 16;          // group types tracked
+constexpr double kLibMinCover = 0.75;             // share of a sweep's ops in library cases to use the kernel
+
+std::string group_key(const QsvSweep &sw, const QsvGroup &g) {
+    std::string k;
+    for (int o = g.op_begin; o < g.op_end; o++) {
+        const QsvOp &op = sw.ops[o];
+        const char c[6] = {(char)op.slot, (char)op.variant, (char)op.kind, (char)op.cls0, (char)op.cls1, (char)op.r00};
+        k.append(c, 6);
+    }
+    return k;
+}
+
+std::string gen_source_lib(const std::vector<std::string> &types, int rb, int wb) {
+    const int nc = 1 << (5 + wb), nt = nc + 32;
+    std::ostringstream s;
+    s << "#include \"qsv_sweep_body.cuh\"\n#include \"qsv_stream.cuh\"\n"
+      << "namespace qsv {\nnamespace dev {\nstruct JitBody {\n"
+      << "    using Amp = float2;\n"
+      << "    static constexpr int kHalfBits = 1;\n"
+      << "    static constexpr bool kSmemOps = true;\n"
+      << "    template <int NV, int RB, int WB>\n"
+      << "    static __device__ __forceinline__ void tile(float2 *tile, const QsvSweep &P, const QsvOp *ops, int lane, int warp,\n"
+      << "                                                int bar) {\n"
+      << "        const int ctid = warp * 32 + lane;\n"
+      << "        const bool swz = P.swz != 0;\n"
+      << "        const int ng = P.ngroups;\n"
+      << "        for (int gi = 0; gi < ng; gi++) {\n"
+      << "            if (gi > 0) named_bar_sync(bar, " << nc << ");\n"
+      << "            const QsvGroup g = P.groups[gi];\n"
+      << "            const bool sin = gi > 0, sout = gi + 1 < ng;\n"
+      << "            const QsvOp *gops = ops + g.op_begin;\n"
+      << "            switch (g.type) {\n";
+    for (size_t t = 0; t < types.size(); t++) {
+        const std::string &k = types[t];
+        s << "            case " << t << ":\n                stream_items_rt<13, " << nc
+          << ">(tile, g, ctid, swz, sin, sout, [&](float2 (&R)[8], float2 (&I)[8], uint32_t x) {\n";
+        for (size_t o = 0; o * 6 < k.size(); o++) {
+            const unsigned char *c = reinterpret_cast<const unsigned char *>(k.data()) + 6 * o;
+            if (c[1] == QSV_V_SKIP) continue;
+            s << "                    stream_op_fixed<true, " << (int)c[0] << ", " << (int)c[1] << ", " << (int)c[2]
+              << ", " << (int)c[3] << ", " << (int)c[4] << ", " << (int)c[5] << ">(gops + " << o << ", R, I, x);\n";
+        }
+        s << "                });\n                break;\n";
+    }
+    s << "            default: {\n"
+      << "                const int n = g.op_end - g.op_begin;\n"
+      << "                stream_items_rt<13, " << nc
+      << ">(tile, g, ctid, swz, sin, sout, [&](float2 (&R)[8], float2 (&I)[8], uint32_t x) {\n"
+      << "                    for (int o = 0; o < n; o++) stream_op<true>(gops + o, R, I, x);\n"
+      << "                });\n                break;\n            }\n"
+      << "            }\n        }\n    }\n};\n}  // namespace dev\n}  // namespace qsv\n"
+      << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", 1)\n"
+      << "    qsv_sweep_jit(float2 *__restrict__ state, const __grid_constant__ QsvSweep P,\n"
+      << "                  const __grid_constant__ CUtensorMap tmap, int *status) {\n"
+      << "    qsv::dev::sweep_pipeline<13, " << rb << ", " << wb << ", " << kStages
       << ", 1, qsv::dev::JitBody, QsvSweep, 0>(state, P, &tmap, status);\n}\n";
     return s.str();
 }
@@ -417,6 +502,14 @@ void worker() {
         j.busy++;
         const std::string src = e->src;
         lk.unlock();
+        // QSV_JIT_DUMP_DIR (tuning): write each generated source there before compiling it
+        if (const char *dir = std::getenv("QSV_JIT_DUMP_DIR")) {
+            const std::string path = std::string(dir) + "/qsv_jit_" + std::to_string(std::hash<std::string>()(src)) + ".cu";
+            if (FILE *f = std::fopen(path.c_str(), "w")) {
+                std::fwrite(src.data(), 1, src.size(), f);
+                std::fclose(f);
+            }
+        }
         std::vector<char> cubin;
         std::string log;
         const auto t0 = std::chrono::steady_clock::now();
@@ -467,9 +560,8 @@ void warm_up_nvrtc() {
 }
 
 // with j.mu held: queue e for compilation (starts the compile threads on first use)
-void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
+void enqueue_src(Jit &j, const std::shared_ptr<Entry> &e) {
     if (e->state != kNew) return;
-    e->src = e->stream ? gen_source_stream(sw, e->rb, e->wb) : gen_source(sw, e->rb, e->wb);
     e->state = kQueued;
     j.queue.push_back(e);
     if (j.stopping) {
@@ -486,6 +578,92 @@ void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
         j.threads = n;
     }
     j.work.notify_one();
+}
+
+void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
+    if (e->state != kNew) return;
+    e->src = e->stream ? gen_source_stream(sw, e->rb, e->wb) : gen_source(sw, e->rb, e->wb);
+    enqueue_src(j, e);
+}
+
+// with j.mu held: adopt a finished library build, forget a failed or dropped one
+void lib_poll(Jit &j) {
+    if (!j.lib_next) return;
+    const State st = j.lib_next->entry->state;
+    if (st == kReady) {
+        j.lib = j.lib_next;
+        j.lib_next = nullptr;
+    } else if (st == kFailed || st == kNew) {
+        j.lib_next = nullptr;
+    }
+}
+
+// with j.mu held: queue a library of `must` (the group types of the sweeps at hand) and then the group types
+// that have swept the most amplitudes, up to kLibMaxTypes cases
+void lib_build(Jit &j, int rb, int wb, const std::vector<std::string> &must) {
+    auto L = std::make_shared<Lib>();
+    L->rb = rb;
+    L->wb = wb;
+    auto add = [&](const std::string &k) {
+        if ((int)L->types.size() < kLibMaxTypes && !L->index.count(k)) {
+            L->index.emplace(k, (int)L->types.size());
+            L->types.push_back(k);
+        }
+    };
+    auto by_weight = [](std::vector<std::pair<double, const std::string *>> &v) {
+        std::sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    };
+    std::vector<std::pair<double, const std::string *>> m, v;
+    for (const std::string &k : must) {
+        auto it = j.gweight.find(k);
+        m.push_back({it != j.gweight.end() ? it->second : 0.0, &k});
+    }
+    by_weight(m);
+    for (auto &p : m) add(*p.second);
+    v.reserve(j.gweight.size());
+    for (auto &kv : j.gweight) v.push_back({kv.second, &kv.first});
+    by_weight(v);
+    for (auto &p : v) add(*p.second);
+    L->entry = std::make_shared<Entry>();
+    L->entry->kw = 13;
+    L->entry->rb = rb;
+    L->entry->wb = wb;
+    L->entry->groups = 1;
+    L->entry->stream = true;
+    L->entry->src = gen_source_lib(L->types, rb, wb);
+    j.lib_next = L;
+    enqueue_src(j, L->entry);
+}
+
+// with j.mu held: give s2's groups their cases in the library in use (type -1: run-time dispatch) and, with
+// work > 0, add work to each group type's swept amplitudes (and the uncovered share to lib_uncovered).
+// Returns the share of the sweep's ops in library cases; keys (if given) receives the group types.
+double lib_annotate(Jit &j, QsvSweep &s2, double work, int rb, int wb, std::vector<std::string> *keys) {
+    const Lib *L = (j.lib && j.lib->rb == rb && j.lib->wb == wb) ? j.lib.get() : nullptr;
+    int total = 0, covered = 0;
+    for (int g = 0; g < s2.ngroups; g++) {
+        QsvGroup &G = s2.groups[g];
+        const std::string k = group_key(s2, G);
+        int n = 0;
+        for (int o = G.op_begin; o < G.op_end; o++) n += s2.ops[o].variant != QSV_V_SKIP;
+        total += n;
+        if (work > 0) {
+            auto it = j.gweight.find(k);
+            if (it != j.gweight.end()) it->second += work;
+            else if (j.gweight.size() < kLibMaxSeen) j.gweight.emplace(k, work);
+        }
+        int idx = -1;
+        if (L) {
+            auto f = L->index.find(k);
+            if (f != L->index.end()) idx = f->second;
+        }
+        G.type = (int16_t)idx;
+        if (idx >= 0) covered += n;
+        if (keys) keys->push_back(k);
+    }
+    const double cover = total ? (double)covered / (double)total : 1.0;
+    if (work > 0) j.lib_uncovered += work * (1.0 - cover);
+    return cover;
 }
 
 std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, bool coarse = false,
@@ -515,7 +693,7 @@ std::shared_ptr<Entry> find_or_add(Jit &j, const QsvSweep &sw, int rb, int wb, b
 }  // namespace
 
 int jit_set_mode(int mode) {
-    if (mode < 0 || mode > 3) return -1;
+    if (mode < 0 || mode > 4) return -1;
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
     const int old = j.mode;
@@ -530,6 +708,36 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
     std::vector<std::shared_ptr<Entry>> mine;
+    if (j.mode == 4 && !stream_form()) {
+        // group-type library: one build (blocking) that covers every group type of the 13-qubit sweeps
+        int rb = 0, wb = 0;
+        layout_for_kw(13, &rb, &wb);
+        std::vector<QsvSweep> s13;
+        std::vector<std::string> keys;
+        bool all = true;
+        for (const QsvSweep &sw : sweeps) {
+            if (sw.kw != 13) continue;
+            s13.push_back(sw);
+            std::string err;
+            if (plan_stream(s13.back(), err) != QSV_OK) { s13.pop_back(); continue; }
+            const double work = (double)sw.ntiles * (double)(1 << sw.kw);
+            all = lib_annotate(j, s13.back(), work, rb, wb, &keys) >= 1.0 && all;
+        }
+        if (!all) {
+            lib_poll(j);
+            if (j.lib_next) {
+                std::shared_ptr<Lib> P = j.lib_next;
+                j.done.wait(lk, [&] { return P->entry->state != kQueued; });
+            }
+            lib_build(j, rb, wb, keys);
+            std::shared_ptr<Lib> L = j.lib_next;
+            j.done.wait(lk, [&] { return L->entry->state != kQueued; });
+            lib_poll(j);
+        }
+        int ready = 0;
+        for (QsvSweep &s2 : s13) ready += lib_annotate(j, s2, 0.0, rb, wb, nullptr) >= 1.0;
+        return ready;
+    }
     for (const QsvSweep &sw : sweeps) {
         int rb = 0, wb = 0;
         if (layout_for_kw(sw.kw, &rb, &wb)) continue;
@@ -563,6 +771,36 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
     return ready;
 }
 
+// Build (blocking) a group-type library from the 13-qubit sweeps of many programs: their group types'
+// swept amplitudes are recorded and the library takes the kLibMaxTypes most swept of every type seen so far.
+// Returns the number of types in the library in use, or -1 if the build failed.
+int jit_prepare_library(const std::vector<QsvSweep> &sweeps) {
+    Jit &j = J();
+    std::unique_lock<std::mutex> lk(j.mu);
+    int rb = 0, wb = 0;
+    layout_for_kw(13, &rb, &wb);
+    QsvSweep s2;
+    for (const QsvSweep &sw : sweeps) {
+        if (sw.kw != 13) continue;
+        std::memcpy(&s2, &sw, sizeof(QsvSweep));
+        std::string err;
+        if (plan_stream(s2, err) != QSV_OK) continue;
+        lib_annotate(j, s2, (double)sw.ntiles * (double)(1 << sw.kw), rb, wb, nullptr);
+    }
+    lib_poll(j);
+    if (j.lib_next) {
+        std::shared_ptr<Lib> P = j.lib_next;
+        j.done.wait(lk, [&] { return P->entry->state != kQueued; });
+    }
+    lib_build(j, rb, wb, {});
+    std::shared_ptr<Lib> L = j.lib_next;
+    j.done.wait(lk, [&] { return L->entry->state != kQueued; });
+    lib_poll(j);
+    j.lib_uncovered = 0.0;
+    if (L->entry->state != kReady) return -1;
+    return (int)j.lib->types.size();
+}
+
 void jit_wait() {
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
@@ -579,12 +817,13 @@ int jit_info(long long *out, int cap) {
         ready += kv.second->state == kReady;
         coarse += kv.second->coarse;
     }
-    const long long v[10] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
+    lib_poll(j);
+    const long long v[12] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
                              (long long)j.compile_ms, (long long)(j.queue.size() + j.busy), j.coarse_launches,
-                             coarse};
-    const int n = std::min(cap, 10);
+                             coarse, j.lib_launches, j.lib ? (long long)j.lib->types.size() : 0};
+    const int n = std::min(cap, 12);
     for (int i = 0; i < n; i++) out[i] = v[i];
-    return 10;
+    return 12;
 }
 
 std::string jit_last_log() {
@@ -608,13 +847,15 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
         if (plan_stream(s2, perr) != QSV_OK) return 0;
     }
     const QsvSweep &sw = sf ? s2 : sw_in;
+    thread_local QsvSweep sl;          // the sweep in streaming form for the group-type library
+    const QsvSweep *lp = &sw;          // what the kernel runs
     const Drv &d = drv();
     std::shared_ptr<Entry> e;
     {
         std::unique_lock<std::mutex> lk(j.mu);
         if (j.mode == 0 || !d.ok) { j.interp_launches++; return 0; }
         const double work = (double)sw.ntiles * (double)(1 << sw.kw);
-        if (j.mode != 3 || sf) {
+        if ((j.mode != 3 && j.mode != 4) || sf) {
             e = find_or_add(j, sw, rb, wb, false, sf);
             e->uses++;
             e->work += work;
@@ -634,6 +875,24 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
                 enqueue(j, ce, c);
             if (j.mode == 3) j.done.wait(lk, [&] { return ce->state != kQueued; });
             if (ce->state == kReady) e = ce;
+        }
+        if ((!e || e->state != kReady) && !sf && sw.kw == 13 && (j.mode == 2 || j.mode == 4)) {
+            // the group-type library, with this sweep's groups annotated with their cases
+            lib_poll(j);
+            std::memcpy(&sl, &sw, sizeof(QsvSweep));
+            std::string perr;
+            if (plan_stream(sl, perr) == QSV_OK) {
+                const double cover = lib_annotate(j, sl, work, rb, wb, nullptr);
+                if (j.lib_uncovered >= kLibThreshold && !j.lib_next && j.queue.size() < kMaxQueued) {
+                    lib_build(j, rb, wb, {});
+                    j.lib_uncovered = 0.0;
+                }
+                if (j.lib && j.lib->rb == rb && j.lib->wb == wb && j.lib->entry->state == kReady &&
+                    cover >= kLibMinCover) {
+                    e = j.lib->entry;
+                    lp = &sl;
+                }
+            }
         }
         if (!e || e->state != kReady) { j.interp_launches++; return 0; }
     }
@@ -670,21 +929,22 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
         e->fn[dev] = fn;
     }
     alignas(64) CUtensorMap map;
-    ce = dev::make_tmap(&map, state, sw);
+    ce = dev::make_tmap(&map, state, *lp);
     if (ce != cudaSuccess) { *err = ce; return -1; }
     int *status = nullptr;
     ce = status_word_ptr(&status);
     if (ce != cudaSuccess) { *err = ce; return -1; }
     int64_t grid = (int64_t)nsm * e->per_sm[dev];
     if (grid > sw.ntiles) grid = sw.ntiles;
-    void *args[] = {&state, const_cast<QsvSweep *>(&sw), &map, &status};
+    void *args[] = {&state, const_cast<QsvSweep *>(lp), &map, &status};
     if (d.launch(e->fn[dev], (unsigned)grid, 1, 1, (unsigned)NT, 1, 1, (unsigned)smem, (CUstream)stream, args,
                  nullptr) != CUDA_SUCCESS) {
         *err = cudaErrorLaunchFailure;
         return -1;
     }
     std::lock_guard<std::mutex> lk(j.mu);
-    j.jit_launches++;
+    if (lp == &sl) j.lib_launches++;
+    else j.jit_launches++;
     if (e->coarse) j.coarse_launches++;
     return 1;
 }

@@ -112,86 +112,91 @@ __device__ __forceinline__ void swap2(float2 &a, float2 &b) {
 // ---------------------------------------------------------------- ops by target slot
 // Register-bit target RBIT: pairs (slot r, slot r | 2^RBIT); each float2 carries two pairs (tile bit 0 =
 // 0 in .x, 1 in .y). One tight unrolled loop per code variant (selected on the host).
-template <int NV, int RBIT, bool IP = false, class O = QsvOp>
-__device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
-                                       const float *m1, bool thread_ok) {
+template <int NV, int RBIT, bool IP, int V, class O>
+__device__ __forceinline__ void reg_case(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
+                                         const float *m1, bool thread_ok) {
     const int cm_reg = op.cm_reg;
 #define QSV_FOR_PAIRS for (int r = 0; r < NV; r++) if (!(r & (1 << RBIT)))
 #define QSV_P1 (r | (1 << RBIT))
-    switch (op.variant) {
-        case QSV_V_UNI_DENSE:
-            if (op.r00) {
+    if constexpr (V == QSV_V_UNI_DENSE) {
+        if (op.r00) {
 #pragma unroll
-                QSV_FOR_PAIRS dense2_r0_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
-            } else {
+            QSV_FOR_PAIRS dense2_r0_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
+        } else {
 #pragma unroll
-                QSV_FOR_PAIRS dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
-            }
-            break;
-        case QSV_V_UNI_DIAG:
-#pragma unroll
-            QSV_FOR_PAIRS { cmul2_t<IP>(R[r], I[r], m0[0], m0[1]); cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m0[6], m0[7]); }
-            break;
-        case QSV_V_UNI_SWAP:
-#pragma unroll
-            QSV_FOR_PAIRS { swap2(R[r], R[QSV_P1]); swap2(I[r], I[QSV_P1]); }
-            break;
-        case QSV_V_CTRL_DENSE:
-#pragma unroll
-            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m1);
-            break;
-        case QSV_V_CTRL_DIAG1:
-#pragma unroll
-            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m1[6], m1[7]);
-            break;
-        case QSV_V_CTRL_SWAP:
-#pragma unroll
-            QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) { swap2(R[r], R[QSV_P1]); swap2(I[r], I[QSV_P1]); }
-            break;
-        case QSV_V_CTRL_DENSE_SEL: {
-            const float id[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f};
-#pragma unroll
-            QSV_FOR_PAIRS {
-                const bool s = thread_ok && (r & cm_reg) == cm_reg;
-                float c[8];
-#pragma unroll
-                for (int e = 0; e < 8; e++) c[e] = s ? m1[e] : id[e];
-                dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
-            }
-            break;
+            QSV_FOR_PAIRS dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m0);
         }
-        case QSV_V_CTRL_DIAG1_SEL:
+    } else if constexpr (V == QSV_V_UNI_DIAG) {
 #pragma unroll
-            QSV_FOR_PAIRS {
-                const bool s = thread_ok && (r & cm_reg) == cm_reg;
-                cmul2_t<IP>(R[QSV_P1], I[QSV_P1], s ? m1[6] : 1.f, s ? m1[7] : 0.f);
-            }
-            break;
-        case QSV_V_CTRL_SWAP_SEL:
+        QSV_FOR_PAIRS { cmul2_t<IP>(R[r], I[r], m0[0], m0[1]); cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m0[6], m0[7]); }
+    } else if constexpr (V == QSV_V_UNI_SWAP) {
 #pragma unroll
-            QSV_FOR_PAIRS {
-                const bool s = thread_ok && (r & cm_reg) == cm_reg;
-                const float2 a = R[r], b = R[QSV_P1], c = I[r], d = I[QSV_P1];
-                R[r] = s ? b : a; R[QSV_P1] = s ? a : b;
-                I[r] = s ? d : c; I[QSV_P1] = s ? c : d;
-            }
-            break;
-        case QSV_V_MUX: {
-            const bool cc = op.cm_c;
+        QSV_FOR_PAIRS { swap2(R[r], R[QSV_P1]); swap2(I[r], I[QSV_P1]); }
+    } else if constexpr (V == QSV_V_CTRL_DENSE) {
 #pragma unroll
-            QSV_FOR_PAIRS {
-                const bool sy = thread_ok && (r & cm_reg) == cm_reg, sx = sy && !cc;
-                float2 c[8];
+        QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], m1);
+    } else if constexpr (V == QSV_V_CTRL_DIAG1) {
 #pragma unroll
-                for (int e = 0; e < 8; e++) c[e] = make_float2(sx ? m1[e] : m0[e], sy ? m1[e] : m0[e]);
-                dense2v(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
-            }
-            break;
+        QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) cmul2_t<IP>(R[QSV_P1], I[QSV_P1], m1[6], m1[7]);
+    } else if constexpr (V == QSV_V_CTRL_SWAP) {
+#pragma unroll
+        QSV_FOR_PAIRS if (thread_ok && (r & cm_reg) == cm_reg) { swap2(R[r], R[QSV_P1]); swap2(I[r], I[QSV_P1]); }
+    } else if constexpr (V == QSV_V_CTRL_DENSE_SEL) {
+        const float id[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f};
+#pragma unroll
+        QSV_FOR_PAIRS {
+            const bool s = thread_ok && (r & cm_reg) == cm_reg;
+            float c[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) c[e] = s ? m1[e] : id[e];
+            dense2_t<IP>(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
         }
-        default: break;
+    } else if constexpr (V == QSV_V_CTRL_DIAG1_SEL) {
+#pragma unroll
+        QSV_FOR_PAIRS {
+            const bool s = thread_ok && (r & cm_reg) == cm_reg;
+            cmul2_t<IP>(R[QSV_P1], I[QSV_P1], s ? m1[6] : 1.f, s ? m1[7] : 0.f);
+        }
+    } else if constexpr (V == QSV_V_CTRL_SWAP_SEL) {
+#pragma unroll
+        QSV_FOR_PAIRS {
+            const bool s = thread_ok && (r & cm_reg) == cm_reg;
+            const float2 a = R[r], b = R[QSV_P1], c = I[r], d = I[QSV_P1];
+            R[r] = s ? b : a; R[QSV_P1] = s ? a : b;
+            I[r] = s ? d : c; I[QSV_P1] = s ? c : d;
+        }
+    } else if constexpr (V == QSV_V_MUX) {
+        const bool cc = op.cm_c;
+#pragma unroll
+        QSV_FOR_PAIRS {
+            const bool sy = thread_ok && (r & cm_reg) == cm_reg, sx = sy && !cc;
+            float2 c[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) c[e] = make_float2(sx ? m1[e] : m0[e], sy ? m1[e] : m0[e]);
+            dense2v(R[r], I[r], R[QSV_P1], I[QSV_P1], c);
+        }
     }
 #undef QSV_FOR_PAIRS
 #undef QSV_P1
+}
+
+// the code path of op.variant, chosen at run time
+template <int NV, int RBIT, bool IP = false, class O = QsvOp>
+__device__ __forceinline__ void reg_op(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
+                                       const float *m1, bool thread_ok) {
+    switch (op.variant) {
+        case QSV_V_UNI_DENSE: reg_case<NV, RBIT, IP, QSV_V_UNI_DENSE>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_UNI_DIAG: reg_case<NV, RBIT, IP, QSV_V_UNI_DIAG>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_UNI_SWAP: reg_case<NV, RBIT, IP, QSV_V_UNI_SWAP>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_DENSE: reg_case<NV, RBIT, IP, QSV_V_CTRL_DENSE>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_DIAG1: reg_case<NV, RBIT, IP, QSV_V_CTRL_DIAG1>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_SWAP: reg_case<NV, RBIT, IP, QSV_V_CTRL_SWAP>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_DENSE_SEL: reg_case<NV, RBIT, IP, QSV_V_CTRL_DENSE_SEL>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_DIAG1_SEL: reg_case<NV, RBIT, IP, QSV_V_CTRL_DIAG1_SEL>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_CTRL_SWAP_SEL: reg_case<NV, RBIT, IP, QSV_V_CTRL_SWAP_SEL>(R, I, op, m0, m1, thread_ok); break;
+        case QSV_V_MUX: reg_case<NV, RBIT, IP, QSV_V_MUX>(R, I, op, m0, m1, thread_ok); break;
+        default: break;
+    }
 }
 
 // tile-bit-0 target: the pair is the two halves of one slot (scalar arithmetic, any variant)
@@ -348,6 +353,28 @@ __device__ __forceinline__ void comp_op_fast(float2 (&R)[NV], float2 (&I)[NV], c
         }
     }
     comp_op<NV, O>(R, I, op, m0, m1, tok);
+}
+
+// comp_op_fast with the kind and matrix classes fixed at compile time (the same code paths)
+template <int NV, int KIND, int CLS0, int CLS1, class O>
+__device__ __forceinline__ void comp_fixed(float2 (&R)[NV], float2 (&I)[NV], const O &op, const float *m0,
+                                           const float *m1, bool tok) {
+    constexpr bool fast = CLS0 == QSV_M_DENSE || CLS0 == QSV_M_DIAG || CLS0 == QSV_M_DIAG1 ||
+                          CLS0 == QSV_M_XSWAP || CLS0 == QSV_M_IDENT;
+    constexpr bool fast1 = CLS1 == QSV_M_DENSE || CLS1 == QSV_M_DIAG || CLS1 == QSV_M_DIAG1 ||
+                           CLS1 == QSV_M_XSWAP || CLS1 == QSV_M_IDENT;
+    if constexpr (KIND == QSV_K_UNI && fast) {
+        if constexpr (CLS0 == QSV_M_DENSE) {
+            if (op.r00) comp_loop<NV, QSV_M_DENSE_R0, false>(R, I, m0, 0, true);
+            else comp_loop<NV, QSV_M_DENSE, false>(R, I, m0, 0, true);
+        } else if constexpr (CLS0 != QSV_M_IDENT) {
+            comp_loop<NV, CLS0, false>(R, I, m0, 0, true);
+        }
+    } else if constexpr (KIND == QSV_K_CTRL && fast1) {
+        if constexpr (CLS1 != QSV_M_IDENT) comp_loop<NV, CLS1, true>(R, I, m1, (int)op.cm_reg, tok);
+    } else {
+        comp_op<NV, O>(R, I, op, m0, m1, tok);
+    }
 }
 
 template <int NV>

@@ -29,6 +29,8 @@
 // compiled at run time by NVRTC (sweep kernels specialised to one structure): no host headers there
 typedef signed char int8_t;
 typedef unsigned char uint8_t;
+typedef short int16_t;
+typedef unsigned short uint16_t;
 typedef int int32_t;
 typedef unsigned int uint32_t;
 typedef long long int64_t;
@@ -154,7 +156,8 @@ struct QsvPhaseX {
 struct QsvGroup {
     uint8_t q[3];               // item bits: distinct, in [1, kw)
     uint8_t op_begin, op_end;
-    uint8_t pad[3];
+    uint8_t pad;
+    int16_t type;               // group-type library: case of this group's op sequence (-1: none)
 };
 
 template <class OpT>

@@ -564,6 +564,7 @@ int plan_stream(QsvSweep &sw, std::string &err) {
         }
         g.op_begin = (uint8_t)i;
         g.op_end = (uint8_t)j;
+        g.type = -1;
         for (int o = i; o < j; o++) {
             QsvOp &op = sw.ops[o];
             const int t = op.tbit;

@@ -112,7 +112,11 @@ __device__ __forceinline__ void stream_op_fixed(const QsvOp *op, float2 (&R)[8],
 #pragma unroll
         for (int e = 0; e < 8; e++) { m0[e] = 0.f; m1[e] = 0.f; }
         op_mats(op, m0, m1, need0, need1);
-        stream_apply<IP>(h, m0, m1, R, I, base);
+        const bool tok = (base & h.cm_thr) == h.cm_thr;
+        if constexpr (SLOT == QSV_SLOT_COMP) comp_fixed<8, KIND, CLS0, CLS1>(R, I, h, m0, m1, tok);
+        else if constexpr (SLOT >= QSV_SLOT_REG0 && SLOT <= QSV_SLOT_REG0 + 2)
+            reg_case<8, SLOT - QSV_SLOT_REG0, IP, VAR>(R, I, h, m0, m1, tok);
+        else if constexpr (SLOT == QSV_SLOT_BASE) base_diag<8, IP>(R, I, h, m0, m1, tok, (base >> h.tbit) & 1u);
     }
 }
 
@@ -153,6 +157,41 @@ __device__ __forceinline__ void stream_items(float2 *tile, const QsvGroup &g, in
         for (int r = 0; r < 8; r++)
             *reinterpret_cast<float4 *>(tile + (sx ^ soff[r])) =
                 SOUT ? make_float4(R[r].x, R[r].y, I[r].x, I[r].y) : make_float4(R[r].x, I[r].x, R[r].y, I[r].y);
+    }
+}
+
+// stream_items with the entry / exit order chosen at run time (selects on the loaded and stored values; one
+// copy of the loop serves every group position)
+template <int KW, int NCG, class F>
+__device__ __forceinline__ void stream_items_rt(float2 *tile, const QsvGroup &g, int ctid, bool swz, bool sin,
+                                                bool sout, F &&body) {
+    const uint32_t q[3] = {g.q[0], g.q[1], g.q[2]};
+    uint32_t soff[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const uint32_t o = ((r & 1) ? 1u << q[0] : 0u) | ((r & 2) ? 1u << q[1] : 0u) | ((r & 4) ? 1u << q[2] : 0u);
+        soff[r] = swz ? swz128(o) : o;
+    }
+    uint32_t s0 = q[0], s1 = q[1], s2 = q[2], t;
+    if (s0 > s1) { t = s0; s0 = s1; s1 = t; }
+    if (s1 > s2) { t = s1; s1 = s2; s2 = t; }
+    if (s0 > s1) { t = s0; s0 = s1; s1 = t; }
+#pragma unroll 1
+    for (int it = ctid; it < (1 << (KW - 4)); it += NCG) {
+        const uint32_t x = insert0(insert0(insert0((uint32_t)it << 1, s0), s1), s2);
+        const uint32_t sx = swz ? swz128(x) : x;
+        float2 R[8], I[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const float4 v = *reinterpret_cast<const float4 *>(tile + (sx ^ soff[r]));
+            R[r] = make_float2(v.x, sin ? v.y : v.z);
+            I[r] = make_float2(sin ? v.z : v.y, v.w);
+        }
+        body(R, I, x);
+#pragma unroll
+        for (int r = 0; r < 8; r++)
+            *reinterpret_cast<float4 *>(tile + (sx ^ soff[r])) =
+                make_float4(R[r].x, sout ? R[r].y : I[r].x, sout ? I[r].x : R[r].y, I[r].y);
     }
 }
 

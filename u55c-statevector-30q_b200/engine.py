@@ -73,6 +73,7 @@ def load(path=LIB_PATH):
         "qsv_inject_skip_load": ([ctypes.c_int], I32),
         "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
         "qsv_jit_wait": ([], I32),
+        "qsv_jit_prepare_library": ([P, P, P, ctypes.c_int], I32),
         "qsv_jit_info": ([P, ctypes.c_int], I32),
         "qsv_hbm_copy": ([P, P, SZ, P], I32),
     }
@@ -97,7 +98,7 @@ def exported_symbols():
             "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_interp", "qsv_set_wait_limit_us",
             "qsv_inject_skip_load", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
-            "qsv_jit_wait", "qsv_jit_info", "qsv_hbm_copy"]
+            "qsv_jit_wait", "qsv_jit_prepare_library", "qsv_jit_info", "qsv_hbm_copy"]
 
 
 def _check(rc):
@@ -353,7 +354,7 @@ def hbm_copy(dst, src, stream=None):
     _check(load().qsv_hbm_copy(_ptr(dst), _ptr(src), nb, _stream(stream)))
 
 
-JIT_MODES = {"off": 0, "eager": 1, "auto": 2, "coarse": 3}
+JIT_MODES = {"off": 0, "eager": 1, "auto": 2, "coarse": 3, "library": 4}
 
 
 def set_wait_limit_us(us):
@@ -370,8 +371,10 @@ def inject_skip_load(count=1):
 def set_jit(mode):
     """Specialised sweep kernels: "off" (interpreter only), "eager" (compile each new sweep structure before
     its first launch), "auto" (default: compile in the background once a structure's launches have swept
-    2^31 amplitudes; meanwhile use the kernel of its coarse structure when that one is ready) or "coarse"
-    (eager, coarse structures only). Values are identical in every mode. Returns the previous mode's name."""
+    2^31 amplitudes; meanwhile use the kernel of its coarse structure or, on 13-qubit windows, the group-type
+    library when ready), "coarse" (eager, coarse structures only) or "library" (the group-type library only;
+    jit_prepare builds it for a segment, jit_prepare_library for many programs). Values are identical in
+    every mode. Returns the previous mode's name."""
     rc = load().qsv_set_jit(JIT_MODES[mode] if isinstance(mode, str) else int(mode))
     if rc < 0:
         _check(rc)
@@ -388,14 +391,29 @@ def jit_prepare(seg, n):
     return rc
 
 
+def jit_prepare_library(programs):
+    """Build (blocking) the group-type library from the 13-qubit sweeps of many programs: `programs` is a
+    list of (segment words, n). Returns the number of group types in the library."""
+    segs = [np.ascontiguousarray(seg, dtype=np.int32) for seg, _ in programs]
+    count = len(segs)
+    ptrs = (ctypes.c_void_p * max(1, count))(*[s.ctypes.data for s in segs])
+    sizes = (ctypes.c_size_t * max(1, count))(*[s.size for s in segs])
+    ns = (ctypes.c_int * max(1, count))(*[int(n) for _, n in programs])
+    rc = load().qsv_jit_prepare_library(ctypes.cast(ptrs, ctypes.c_void_p), ctypes.cast(sizes, ctypes.c_void_p),
+                                        ctypes.cast(ns, ctypes.c_void_p), count)
+    if rc < 0:
+        _check(rc)
+    return rc
+
+
 def jit_wait():
     _check(load().qsv_jit_wait())
 
 
 def jit_info():
     """Counters of the specialised-kernel cache."""
-    buf = (ctypes.c_longlong * 10)()
-    load().qsv_jit_info(ctypes.cast(buf, ctypes.c_void_p), 10)
+    buf = (ctypes.c_longlong * 12)()
+    load().qsv_jit_info(ctypes.cast(buf, ctypes.c_void_p), 12)
     keys = ["mode", "structures", "ready", "failed", "jit_launches", "interp_launches", "compile_ms", "pending",
-            "coarse_launches", "coarse_structures"]
+            "coarse_launches", "coarse_structures", "lib_launches", "lib_types"]
     return dict(zip(keys, [int(x) for x in buf]))
