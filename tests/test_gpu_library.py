@@ -107,3 +107,25 @@ def test_prepare_library_rejects_bad_segments(torch):
         engine.jit_prepare_library([(np.zeros(4, dtype=np.int32), 20)])
     with pytest.raises(Exception):
         engine.jit_prepare_library([(np.zeros(4, dtype=np.int32), 40)])
+
+
+@pytest.mark.timeout(900)
+def test_library_serves_sweeps_planned_in_either_layout(torch):
+    """The streaming form does not depend on the phase layouts: a library built while 13-qubit sweeps use 4
+    register bits per thread serves them when they are planned with 3 (16 consumer warps), launched with
+    the block it was compiled for; values stay exact."""
+    n = 19
+    prog, _, _ = q.compile_circuit(gen.random_layer_ccx(n, 6, 71), n, 12)
+    old = engine.set_jit("library")
+    try:
+        engine.set_layout13(4)
+        engine.jit_prepare_library([(seg, n) for kind, seg in prog if kind == "segment"])
+        engine.set_layout13(3)
+        before = engine.jit_info()
+        y, ref = _run(torch, prog, _rand_state(n, 78))
+        after = engine.jit_info()
+    finally:
+        engine.set_layout13(4)
+        engine.set_jit(old)
+    assert np.array_equal(y, ref), f"max diff {np.max(np.abs(y - ref))}"
+    assert after["lib_launches"] > before["lib_launches"]

@@ -639,7 +639,8 @@ void lib_build(Jit &j, int rb, int wb, const std::vector<std::string> &must) {
 // work > 0, add work to each group type's swept amplitudes (and the uncovered share to lib_uncovered).
 // Returns the share of the sweep's ops in library cases; keys (if given) receives the group types.
 double lib_annotate(Jit &j, QsvSweep &s2, double work, int rb, int wb, std::vector<std::string> *keys) {
-    const Lib *L = (j.lib && j.lib->rb == rb && j.lib->wb == wb) ? j.lib.get() : nullptr;
+    (void)rb; (void)wb;
+    const Lib *L = j.lib.get();         // the streaming form does not depend on the phase layouts
     int total = 0, covered = 0;
     for (int g = 0; g < s2.ngroups; g++) {
         QsvGroup &G = s2.groups[g];
@@ -887,8 +888,7 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
                     lib_build(j, rb, wb, {});
                     j.lib_uncovered = 0.0;
                 }
-                if (j.lib && j.lib->rb == rb && j.lib->wb == wb && j.lib->entry->state == kReady &&
-                    cover >= kLibMinCover) {
+                if (j.lib && j.lib->entry->state == kReady && cover >= kLibMinCover) {
                     e = j.lib->entry;
                     lp = &sl;
                 }
@@ -899,7 +899,8 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) { *err = ce != cudaSuccess ? ce : cudaErrorInvalidDevice; return -1; }
-    const int NT = e->groups * (1 << (5 + wb)) + 32;
+    // the block the kernel was compiled for (a library kernel keeps the layout it was built with)
+    const int NT = e->groups * (1 << (5 + e->wb)) + 32;
     // sweep_smem_bytes of the generated body: the tile buffers plus 1 KiB for their 1024-byte alignment
     const size_t smem = ((size_t)kStages << sw.kw) * sizeof(float2) + QSV_SMEM_ALIGN +
                         (e->stream ? sizeof(QsvOp) * QSV_MAX_SWEEP_OPS : 0);

@@ -568,6 +568,11 @@ int plan_stream(QsvSweep &sw, std::string &err) {
         for (int o = i; o < j; o++) {
             QsvOp &op = sw.ops[o];
             const int t = op.tbit;
+            // the branch-free controlled forms (chosen for lane-bit controls of a phase layout) give the
+            // same values as the plain ones, which skip unselected pairs: items have no lane bits
+            if (op.variant == QSV_V_CTRL_DENSE_SEL) op.variant = QSV_V_CTRL_DENSE;
+            else if (op.variant == QSV_V_CTRL_DIAG1_SEL) op.variant = QSV_V_CTRL_DIAG1;
+            else if (op.variant == QSV_V_CTRL_SWAP_SEL) op.variant = QSV_V_CTRL_SWAP;
             op.slot = QSV_SLOT_BASE;
             if (t == 0) op.slot = QSV_SLOT_COMP;
             op.cm_reg = 0;
