@@ -190,11 +190,12 @@ QSV_API int qsv_set_phase_lanes(int k);
  * coarse structure's kernel, compiled once the sweeps sharing it have swept 2^30 amplitudes, or (13-qubit
  * windows) the group-type library, or the interpreter; 3 = eager with coarse structures only; 4 = the
  * group-type library only (qsv_jit_prepare builds it, blocking, to cover a segment's 13-qubit sweeps).
- * The group-type library is one kernel holding straight-line code for up to 32 op sequences of one group
- * of the streaming form (per op: slot among the group's three item bits, code variant, kind, matrix
- * classes), the ones that have swept the most amplitudes, with item bits, control masks and matrices read
- * at run time; it serves sweeps whose exact and coarse structures never repeat once 3/4 of their ops fall
- * in its cases, and is rebuilt in the background after groups outside it have swept 2^31 amplitudes.
+ * The group-type library is a set of up to 8 kernels, each with straight-line code for 32 op sequences of
+ * one group of the streaming form (per op: slot among the group's three item bits, code variant, kind,
+ * matrix classes): the 16 that have swept the most amplitudes and a band of 16 more, with item bits,
+ * control masks and matrices read at run time. A sweep whose exact and coarse structures never repeat
+ * takes the kernel that covers most of its ops, once 3/4 of them fall in its cases; the set is rebuilt in
+ * the background after groups outside it have swept 2^31 amplitudes.
  * Switching to mode 0 drops waiting compilations and waits for running ones. Returns the previous mode.
  * Process-wide. */
 QSV_API int qsv_set_jit(int mode);
@@ -207,7 +208,7 @@ QSV_API int qsv_jit_prepare(const int32_t *seg, size_t nwords, int n);
 
 /* Build (blocking, host work only) the group-type library (qsv_set_jit) from the 13-qubit sweeps of count
  * programs (segment i: segs[i], nwords[i] words, for an ns[i]-qubit state): their group types' swept
- * amplitudes are recorded and the library takes the 32 most swept types seen so far. A batch or a service
+ * amplitudes are recorded and the libraries take the most swept types seen so far (up to 144). A batch or a service
  * calls it once before its timed or latency-bound work. Returns the number of types in the library, or a
  * negative error code (malformed segment; QSV_ERR_CUDA if the library does not compile). */
 QSV_API int qsv_jit_prepare_library(const int32_t *const *segs, const size_t *nwords, const int *ns, int count);

@@ -1,7 +1,7 @@
 """The group-type library kernel gives the C oracle's values exactly.
 
-The library (qsv_set_jit mode 4, "library") is one kernel for 13-qubit windows with straight-line code for
-up to 32 group types of the streaming form (per op: slot among the group's item bits, variant, kind, matrix
+The library (qsv_set_jit mode 4, "library") is a set of kernels for 13-qubit windows (up to 8, each with the
+16 most swept group types and a band of 16 more), each with straight-line code for its group types of the streaming form (per op: slot among the group's item bits, variant, kind, matrix
 classes) and a run-time-dispatch path for groups of other types; item bits, control masks and matrices are
 read at run time. Its cases and its fallback run the interpreter's per-variant arithmetic, so every value
 equals the oracle's (np.array_equal: signs of zeros aside). Cases: random layers with Toffolis (controls on
@@ -77,7 +77,7 @@ def test_library_exact_vs_oracle(torch, n, k, maker):
     finally:
         engine.set_jit(old)
     assert np.array_equal(y, ref), f"n={n}: max diff {np.max(np.abs(y - ref))}"
-    assert 0 < after["lib_types"] <= 32
+    assert 0 < after["lib_types"] <= 144
     assert after["lib_launches"] > before["lib_launches"]
 
 
@@ -91,7 +91,7 @@ def test_library_from_other_programs_with_fallback_groups(torch):
     old = engine.set_jit("library")
     try:
         types = engine.jit_prepare_library(segs0)
-        assert 0 < types <= 32
+        assert 0 < types <= 144
         before = engine.jit_info()
         y, ref = _run(torch, progs[1], _rand_state(n, 77))
         after = engine.jit_info()

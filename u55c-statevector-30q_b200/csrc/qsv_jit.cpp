@@ -163,6 +163,12 @@ struct Lib {
     std::shared_ptr<Entry> entry;
 };
 
+// the libraries of one build
+struct LibSet {
+    std::vector<std::shared_ptr<Lib>> libs;
+    int types = 0;              // distinct group types over the libraries
+};
+
 struct Jit {
     std::mutex mu;
     std::condition_variable work, done;
@@ -174,7 +180,7 @@ struct Jit {
     long long jit_launches = 0, interp_launches = 0, coarse_launches = 0, compiled = 0, failed = 0;
     // group-type library: amplitudes swept per group type, the library in use and the one being built
     std::unordered_map<std::string, double> gweight;
-    std::shared_ptr<Lib> lib, lib_next;
+    std::shared_ptr<LibSet> lib, lib_next;
     double lib_uncovered = 0.0;
     long long lib_launches = 0;
     double compile_ms = 0.0;
@@ -306,9 +312,12 @@ std::string gen_source_stream(const QsvSweep &sw, int rb, int wb) {
 // is ONE kernel for 13-qubit windows with straight-line code for each of up to kLibMaxTypes group types and
 // a run-time-dispatch path for the others; it is rebuilt, in the background, from the types that have
 // swept the most amplitudes. Item bits, control masks and matrices are read at run time.
-constexpr int kLibMaxTypes = 32;        // front-end compile time grows faster than linearly with the cases
-                                        // (10 / 20 / 40 / 86 cases: 4 / 7 / 17 / ~80 s); the 16 / 64 most
-                                        // swept group types cover 87 / 94 % of the groups of a mixed batch
+// A library holds kLibCommon + kLibBand cases: front-end compile time grows faster than linearly with the
+// cases (10 / 20 / 40 / 86 cases: 4 / 7 / 17 / ~80 s), so wider coverage comes from several libraries
+// compiled in parallel. The 16 / 64 most swept group types cover 87 / 94 % of the groups of a mixed batch.
+constexpr int kLibCommon = 16;          // the most swept types, in every library
+constexpr int kLibBand = 16;            // then a band of its own
+constexpr int kLibSets = 8;             // libraries per build
 constexpr double kLibThreshold = 2147483648.0;   // amplitudes swept by groups outside the library before a rebuild
 constexpr size_t kLibMaxSeen = 1u << 16;          // group types tracked
 constexpr double kLibMinCover = 0.75;             // share of a sweep's ops in library cases to use the kernel
@@ -586,32 +595,43 @@ void enqueue(Jit &j, const std::shared_ptr<Entry> &e, const QsvSweep &sw) {
     enqueue_src(j, e);
 }
 
-// with j.mu held: adopt a finished library build, forget a failed or dropped one
+// with j.mu held: adopt a finished build (the libraries of it that compiled), forget a dropped one
 void lib_poll(Jit &j) {
     if (!j.lib_next) return;
-    const State st = j.lib_next->entry->state;
-    if (st == kReady) {
-        j.lib = j.lib_next;
-        j.lib_next = nullptr;
-    } else if (st == kFailed || st == kNew) {
-        j.lib_next = nullptr;
+    for (auto &L : j.lib_next->libs)
+        if (L->entry->state == kQueued) return;               // still compiling
+    auto done = std::make_shared<LibSet>();
+    for (auto &L : j.lib_next->libs)
+        if (L->entry->state == kReady) done->libs.push_back(L);
+    if (!done->libs.empty()) {
+        std::unordered_map<std::string, int> all;
+        for (auto &L : done->libs)
+            for (auto &k : L->types) all.emplace(k, 0);
+        done->types = (int)all.size();
+        j.lib = done;
     }
+    j.lib_next = nullptr;
 }
 
-// with j.mu held: queue a library of `must` (the group types of the sweeps at hand) and then the group types
-// that have swept the most amplitudes, up to kLibMaxTypes cases
+bool lib_building(Jit &j) {
+    if (!j.lib_next) return false;
+    for (auto &L : j.lib_next->libs)
+        if (L->entry->state == kQueued) return true;
+    return false;
+}
+
+// with j.mu held: queue a build. The group types are ranked by swept amplitudes, `must` (the types of the
+// sweeps at hand) first; the kLibCommon first ones go into every library, each library adds its own band of
+// the next kLibBand, up to kLibSets libraries compiled in parallel (a sweep takes the one that covers most
+// of its ops, so its common groups and one rarer group are covered together).
 void lib_build(Jit &j, int rb, int wb, const std::vector<std::string> &must) {
-    auto L = std::make_shared<Lib>();
-    L->rb = rb;
-    L->wb = wb;
-    auto add = [&](const std::string &k) {
-        if ((int)L->types.size() < kLibMaxTypes && !L->index.count(k)) {
-            L->index.emplace(k, (int)L->types.size());
-            L->types.push_back(k);
-        }
-    };
+    std::vector<std::string> ranked;
+    std::unordered_map<std::string, int> seen;
     auto by_weight = [](std::vector<std::pair<double, const std::string *>> &v) {
         std::sort(v.begin(), v.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    };
+    auto add = [&](const std::string &k) {
+        if (!seen.count(k)) { seen.emplace(k, 0); ranked.push_back(k); }
     };
     std::vector<std::pair<double, const std::string *>> m, v;
     for (const std::string &k : must) {
@@ -624,44 +644,77 @@ void lib_build(Jit &j, int rb, int wb, const std::vector<std::string> &must) {
     for (auto &kv : j.gweight) v.push_back({kv.second, &kv.first});
     by_weight(v);
     for (auto &p : v) add(*p.second);
-    L->entry = std::make_shared<Entry>();
-    L->entry->kw = 13;
-    L->entry->rb = rb;
-    L->entry->wb = wb;
-    L->entry->groups = 1;
-    L->entry->stream = true;
-    L->entry->src = gen_source_lib(L->types, rb, wb);
-    j.lib_next = L;
-    enqueue_src(j, L->entry);
+    auto set = std::make_shared<LibSet>();
+    const size_t common = std::min(ranked.size(), (size_t)kLibCommon);
+    for (int b = 0; b < kLibSets; b++) {
+        const size_t lo = common + (size_t)b * kLibBand;
+        if (b > 0 && lo >= ranked.size()) break;
+        auto L = std::make_shared<Lib>();
+        L->rb = rb;
+        L->wb = wb;
+        auto put = [&](const std::string &k) {
+            if (!L->index.count(k)) { L->index.emplace(k, (int)L->types.size()); L->types.push_back(k); }
+        };
+        for (size_t i = 0; i < common; i++) put(ranked[i]);
+        for (size_t i = lo; i < std::min(ranked.size(), lo + kLibBand); i++) put(ranked[i]);
+        L->entry = std::make_shared<Entry>();
+        L->entry->kw = 13;
+        L->entry->rb = rb;
+        L->entry->wb = wb;
+        L->entry->groups = 1;
+        L->entry->stream = true;
+        L->entry->src = gen_source_lib(L->types, rb, wb);
+        set->libs.push_back(L);
+    }
+    j.lib_next = set;
+    for (auto &L : set->libs) enqueue_src(j, L->entry);
 }
 
-// with j.mu held: give s2's groups their cases in the library in use (type -1: run-time dispatch) and, with
-// work > 0, add work to each group type's swept amplitudes (and the uncovered share to lib_uncovered).
-// Returns the share of the sweep's ops in library cases; keys (if given) receives the group types.
-double lib_annotate(Jit &j, QsvSweep &s2, double work, int rb, int wb, std::vector<std::string> *keys) {
-    (void)rb; (void)wb;
-    const Lib *L = j.lib.get();         // the streaming form does not depend on the phase layouts
-    int total = 0, covered = 0;
+// with j.mu held: wait (j.done) until the build in progress has finished, then adopt it
+void lib_wait(Jit &j, std::unique_lock<std::mutex> &lk) {
+    j.done.wait(lk, [&] { return !lib_building(j); });
+    lib_poll(j);
+}
+
+// with j.mu held: give s2's groups their cases in the library (of those in use) that covers most of its ops
+// (type -1: run-time dispatch) and, with work > 0, add work to each group type's swept amplitudes (and the
+// uncovered share to lib_uncovered). Returns the share of the sweep's ops in that library's cases (*best:
+// the library, or null); keys (if given) receives the group types.
+double lib_annotate(Jit &j, QsvSweep &s2, double work, std::vector<std::string> *keys, const Lib **best) {
+    std::string k[QSV_MAX_GROUPS];
+    int n[QSV_MAX_GROUPS], total = 0;
     for (int g = 0; g < s2.ngroups; g++) {
-        QsvGroup &G = s2.groups[g];
-        const std::string k = group_key(s2, G);
-        int n = 0;
-        for (int o = G.op_begin; o < G.op_end; o++) n += s2.ops[o].variant != QSV_V_SKIP;
-        total += n;
+        const QsvGroup &G = s2.groups[g];
+        k[g] = group_key(s2, G);
+        n[g] = 0;
+        for (int o = G.op_begin; o < G.op_end; o++) n[g] += s2.ops[o].variant != QSV_V_SKIP;
+        total += n[g];
         if (work > 0) {
-            auto it = j.gweight.find(k);
+            auto it = j.gweight.find(k[g]);
             if (it != j.gweight.end()) it->second += work;
-            else if (j.gweight.size() < kLibMaxSeen) j.gweight.emplace(k, work);
+            else if (j.gweight.size() < kLibMaxSeen) j.gweight.emplace(k[g], work);
         }
+        if (keys) keys->push_back(k[g]);
+    }
+    // the streaming form does not depend on the phase layouts: any library serves any 13-qubit sweep
+    const Lib *L = nullptr;
+    int covered = 0;
+    if (j.lib) {
+        for (auto &C : j.lib->libs) {
+            int c = 0;
+            for (int g = 0; g < s2.ngroups; g++) c += C->index.count(k[g]) ? n[g] : 0;
+            if (!L || c > covered) { L = C.get(); covered = c; }
+        }
+    }
+    for (int g = 0; g < s2.ngroups; g++) {
         int idx = -1;
         if (L) {
-            auto f = L->index.find(k);
+            auto f = L->index.find(k[g]);
             if (f != L->index.end()) idx = f->second;
         }
-        G.type = (int16_t)idx;
-        if (idx >= 0) covered += n;
-        if (keys) keys->push_back(k);
+        s2.groups[g].type = (int16_t)idx;
     }
+    if (best) *best = L;
     const double cover = total ? (double)covered / (double)total : 1.0;
     if (work > 0) j.lib_uncovered += work * (1.0 - cover);
     return cover;
@@ -722,21 +775,15 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
             std::string err;
             if (plan_stream(s13.back(), err) != QSV_OK) { s13.pop_back(); continue; }
             const double work = (double)sw.ntiles * (double)(1 << sw.kw);
-            all = lib_annotate(j, s13.back(), work, rb, wb, &keys) >= 1.0 && all;
+            all = lib_annotate(j, s13.back(), work, &keys, nullptr) >= 1.0 && all;
         }
         if (!all) {
-            lib_poll(j);
-            if (j.lib_next) {
-                std::shared_ptr<Lib> P = j.lib_next;
-                j.done.wait(lk, [&] { return P->entry->state != kQueued; });
-            }
+            lib_wait(j, lk);
             lib_build(j, rb, wb, keys);
-            std::shared_ptr<Lib> L = j.lib_next;
-            j.done.wait(lk, [&] { return L->entry->state != kQueued; });
-            lib_poll(j);
+            lib_wait(j, lk);
         }
         int ready = 0;
-        for (QsvSweep &s2 : s13) ready += lib_annotate(j, s2, 0.0, rb, wb, nullptr) >= 1.0;
+        for (QsvSweep &s2 : s13) ready += lib_annotate(j, s2, 0.0, nullptr, nullptr) >= 1.0;
         return ready;
     }
     for (const QsvSweep &sw : sweeps) {
@@ -786,20 +833,16 @@ int jit_prepare_library(const std::vector<QsvSweep> &sweeps) {
         std::memcpy(&s2, &sw, sizeof(QsvSweep));
         std::string err;
         if (plan_stream(s2, err) != QSV_OK) continue;
-        lib_annotate(j, s2, (double)sw.ntiles * (double)(1 << sw.kw), rb, wb, nullptr);
+        lib_annotate(j, s2, (double)sw.ntiles * (double)(1 << sw.kw), nullptr, nullptr);
     }
-    lib_poll(j);
-    if (j.lib_next) {
-        std::shared_ptr<Lib> P = j.lib_next;
-        j.done.wait(lk, [&] { return P->entry->state != kQueued; });
-    }
+    lib_wait(j, lk);
     lib_build(j, rb, wb, {});
-    std::shared_ptr<Lib> L = j.lib_next;
-    j.done.wait(lk, [&] { return L->entry->state != kQueued; });
-    lib_poll(j);
+    const std::shared_ptr<LibSet> built = j.lib_next;
+    lib_wait(j, lk);
     j.lib_uncovered = 0.0;
-    if (L->entry->state != kReady) return -1;
-    return (int)j.lib->types.size();
+    for (auto &L : built->libs)
+        if (L->entry->state != kReady) return -1;
+    return j.lib ? j.lib->types : 0;
 }
 
 void jit_wait() {
@@ -821,7 +864,7 @@ int jit_info(long long *out, int cap) {
     lib_poll(j);
     const long long v[12] = {j.mode, (long long)j.map.size(), ready, j.failed, j.jit_launches, j.interp_launches,
                              (long long)j.compile_ms, (long long)(j.queue.size() + j.busy), j.coarse_launches,
-                             coarse, j.lib_launches, j.lib ? (long long)j.lib->types.size() : 0};
+                             coarse, j.lib_launches, j.lib ? (long long)j.lib->types : 0};
     const int n = std::min(cap, 12);
     for (int i = 0; i < n; i++) out[i] = v[i];
     return 12;
@@ -883,13 +926,14 @@ int jit_try_launch(float2 *state, const QsvSweep &sw_in, int nsm, cudaStream_t s
             std::memcpy(&sl, &sw, sizeof(QsvSweep));
             std::string perr;
             if (plan_stream(sl, perr) == QSV_OK) {
-                const double cover = lib_annotate(j, sl, work, rb, wb, nullptr);
+                const Lib *best = nullptr;
+                const double cover = lib_annotate(j, sl, work, nullptr, &best);
                 if (j.lib_uncovered >= kLibThreshold && !j.lib_next && j.queue.size() < kMaxQueued) {
                     lib_build(j, rb, wb, {});
                     j.lib_uncovered = 0.0;
                 }
-                if (j.lib && j.lib->entry->state == kReady && cover >= kLibMinCover) {
-                    e = j.lib->entry;
+                if (best && best->entry->state == kReady && cover >= kLibMinCover) {
+                    e = best->entry;
                     lp = &sl;
                 }
             }
