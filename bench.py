@@ -356,6 +356,16 @@ def served_main(a):
             out.append(x)
         return out
 
+    # group-type libraries for the 13-qubit sweeps, from up to 400 sampled requests (a service builds them at
+    # start-up from its recent requests; both sides use them)
+    lib_info = None
+    if a.jit in ("auto", "library") and not a.compile_on_arrival:
+        t0 = time.perf_counter()
+        pick = base if len(base) <= 400 else [base[i] for i in np.random.default_rng(1).choice(len(base), 400,
+                                                                                              replace=False)]
+        big = [(seg, r.n) for r in pick if r.n > 13 for seg in r.program]
+        lib_info = {"types": engine.jit_prepare_library(big) if big else 0,
+                    "build_s": round(time.perf_counter() - t0, 2)}
     srv = serve.Server(budget_bytes=160e9, max_inflight=16, policy=a.policy,
                        compile_workers=workers if a.compile_on_arrival else 0)
     srv.warm()                      # compile workers started before the arrivals (service start-up)
@@ -404,7 +414,7 @@ def served_main(a):
                       "qubits": {"min": int(min(ns)), "max": int(max(ns)), "count_30": int(sum(x == 30 for x in ns))},
                       "algorithmic_bytes": work_bytes or None, "algorithmic_bytes_kind": work_kind,
                       "hbm_floor_s": (work_bytes / (_peaks()[0] * 1e9)) if work_bytes else None,
-                      "host_compile_s": t_compile, "rates": per_rate,
+                      "host_compile_s": t_compile, "group_library": lib_info, "rates": per_rate,
                       "speedup_vs_plain": top["speedup_vs_plain"],
                       "results_identical_alone_and_in_mix": equal_all, "clocks": clk.summary()}))
 
