@@ -131,6 +131,14 @@ QSV_API int qsv_batch_launch(qsv_batch *batch, void *workspace, size_t bytes, vo
  * the number of words of the full plan, or a negative error code. Pure host code, no device work. */
 QSV_API int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap);
 
+/* The streaming form of the same sweeps (no reference counterpart): how the streaming interpreter and the
+ * group-type library run them. Writes at most `cap` int32 words: the sweep count, then per sweep kw,
+ * ngroups, nops, per group its three item bits and op range, per op tbit, slot (0 = tile bit 0, 1 + k =
+ * item bit k, 7 = a base bit, diagonal ops only), variant, cmask, cm_reg (controls on item bits), cm_thr
+ * (controls on base bits), kind. Returns the number of words of the full plan, or a negative error code.
+ * Pure host code. */
+QSV_API int qsv_plan_stream(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap);
+
 /* HBM copy probe: dst <- src, `bytes` (a multiple of 16, 16-byte aligned, not overlapping), a grid-stride
  * 16-byte copy that reads and writes every byte once. The measured achievable-bandwidth denominator for the
  * sweep roofline; the B200 counterpart of the reference's FPGA HBM stream microbenchmark

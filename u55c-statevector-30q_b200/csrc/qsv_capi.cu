@@ -137,6 +137,23 @@ int qsv_plan_segment(const int32_t *seg, size_t nwords, int n, int32_t *out, siz
     return qsv::serialize(sweeps, out, cap);
 }
 
+int qsv_plan_stream(const int32_t *seg, size_t nwords, int n, int32_t *out, size_t cap) {
+    if (n < QSV_N_MIN || n > QSV_N_MAX) return fail(QSV_ERR_INVALID_ARG, "n out of [10, 34]");
+    std::vector<qsv::PhysPass> passes;
+    std::string err;
+    int rc = qsv::decode_segment(seg, nwords, n, passes, err);
+    if (rc) return fail(rc, err);
+    std::vector<QsvSweep> sweeps;
+    const int kw = n < QSV_KW_MAX ? n : QSV_KW_MAX;
+    rc = qsv::build_sweeps<QsvOp>(passes, n, kw, g_lo_merge, sweeps, err);
+    if (rc) return fail(rc, err);
+    for (QsvSweep &sw : sweeps) {
+        rc = qsv::plan_stream(sw, err);
+        if (rc) return fail(rc, err);
+    }
+    return qsv::serialize_stream(sweeps, out, cap);
+}
+
 int qsv_run_segment(void *state, int n, const int32_t *seg, size_t nwords, int dtype, void *stream) {
     if (!state) return fail(QSV_ERR_INVALID_ARG, "state is null");
     if (!dtype_ok(dtype)) return fail(QSV_ERR_UNSUPPORTED, "dtype must be QSV_C64 or QSV_C128");

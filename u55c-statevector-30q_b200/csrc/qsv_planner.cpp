@@ -588,6 +588,26 @@ int plan_stream(QsvSweep &sw, std::string &err) {
     return QSV_OK;
 }
 
+int serialize_stream(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
+    std::vector<int32_t> w;
+    w.push_back((int32_t)sw.size());
+    for (const QsvSweep &s : sw) {
+        w.push_back(s.kw); w.push_back(s.ngroups); w.push_back(s.nops);
+        for (int g = 0; g < s.ngroups; g++) {
+            const QsvGroup &G = s.groups[g];
+            for (int k = 0; k < 3; k++) w.push_back(G.q[k]);
+            w.push_back(G.op_begin); w.push_back(G.op_end);
+        }
+        for (int o = 0; o < s.nops; o++) {
+            const QsvOp &op = s.ops[o];
+            w.push_back(op.tbit); w.push_back(op.slot); w.push_back(op.variant); w.push_back((int32_t)op.cmask);
+            w.push_back(op.cm_reg); w.push_back((int32_t)op.cm_thr); w.push_back(op.kind);
+        }
+    }
+    if (out) std::memcpy(out, w.data(), sizeof(int32_t) * std::min(cap, w.size()));
+    return (int)w.size();
+}
+
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap) {
     std::vector<int32_t> w;
     w.push_back((int32_t)sw.size());

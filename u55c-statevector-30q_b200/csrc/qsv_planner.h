@@ -55,6 +55,9 @@ int plan_whole_state(const std::vector<PhysPass> &passes, int n, std::vector<Qsv
 // distinct target tile bits >= 1 (ops on tile bit 0 and diagonal ops on other bits join any group), and
 // each op's slot / control split for its group's item layout. Replaces the phase fields of the ops.
 int plan_stream(QsvSweep &sw, std::string &err);
+// Flatten streaming plans (plan_stream) into int32 words: sweeps; per sweep kw, ngroups, nops, then per group
+// q0 q1 q2 op_begin op_end, then per op tbit slot variant cmask cm_reg cm_thr kind.
+int serialize_stream(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap);
 // Flatten a plan into int32 words (layout documented in qsv_b200.h / the planner tests).
 int serialize(const std::vector<QsvSweep> &sw, int32_t *out, size_t cap);
 

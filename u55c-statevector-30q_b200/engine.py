@@ -73,6 +73,7 @@ def load(path=LIB_PATH):
         "qsv_inject_skip_load": ([ctypes.c_int], I32),
         "qsv_jit_prepare": ([P, SZ, ctypes.c_int], I32),
         "qsv_jit_wait": ([], I32),
+        "qsv_plan_stream": ([P, SZ, ctypes.c_int, P, SZ], I32),
         "qsv_jit_prepare_library": ([P, P, P, ctypes.c_int], I32),
         "qsv_jit_info": ([P, ctypes.c_int], I32),
         "qsv_hbm_copy": ([P, P, SZ, P], I32),
@@ -94,7 +95,7 @@ def exported_symbols():
     return ["qsv_version", "qsv_last_error", "qsv_run_segment", "qsv_remap", "qsv_zero_state",
             "qsv_reduce_scratch_bytes", "qsv_reduce_f64", "qsv_reduce_f64_noalloc", "qsv_chunk_probs_f64",
             "qsv_sample_f64",
-            "qsv_plan_segment", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
+            "qsv_plan_segment", "qsv_plan_stream", "qsv_device_status", "qsv_take_launch_count", "qsv_set_lo_merge",
             "qsv_set_layout13", "qsv_set_phase_lanes", "qsv_set_interp", "qsv_set_wait_limit_us",
             "qsv_inject_skip_load", "qsv_batch_new", "qsv_batch_free", "qsv_batch_add",
             "qsv_batch_workspace_bytes", "qsv_batch_upload", "qsv_batch_launch", "qsv_set_jit", "qsv_jit_prepare",
@@ -232,6 +233,35 @@ def plan_segment(seg, n):
     buf = np.zeros(need, dtype=np.int32)
     L.qsv_plan_segment(w.ctypes.data_as(ctypes.c_void_p), w.size, n, buf.ctypes.data_as(ctypes.c_void_p), need)
     return _parse_plan(buf, n)
+
+
+def plan_stream(seg, n):
+    """The streaming form of a segment's sweeps (host only): per sweep a dict with kw, its groups (item bits
+    q, op range) and per op the slot and control split in that form."""
+    L = load()
+    w = np.ascontiguousarray(seg, dtype=np.int32)
+    need = L.qsv_plan_stream(w.ctypes.data_as(ctypes.c_void_p), w.size, n, None, 0)
+    if need < 0:
+        _check(need)
+    buf = np.zeros(need, dtype=np.int32)
+    L.qsv_plan_stream(w.ctypes.data_as(ctypes.c_void_p), w.size, n, buf.ctypes.data_as(ctypes.c_void_p), need)
+    pos, out = 1, []
+    for _ in range(int(buf[0])):
+        kw, ng, nops = (int(x) for x in buf[pos:pos + 3])
+        pos += 3
+        groups = []
+        for _ in range(ng):
+            r = [int(x) for x in buf[pos:pos + 5]]
+            pos += 5
+            groups.append(dict(q=r[:3], op_begin=r[3], op_end=r[4]))
+        ops = []
+        for _ in range(nops):
+            tbit, slot, variant, cmask, cm_reg, cm_thr, kind = (int(x) for x in buf[pos:pos + 7])
+            pos += 7
+            ops.append(dict(tbit=tbit, slot=slot, variant=variant, cmask=cmask & 0xFFFFFFFF, cm_reg=cm_reg,
+                            cm_thr=cm_thr & 0xFFFFFFFF, kind=kind))
+        out.append(dict(kw=kw, groups=groups, ops=ops))
+    return out
 
 
 def _parse_plan(w, n):
