@@ -111,3 +111,22 @@ def test_group_type_library_compiles(lib):
         engine.set_jit(old)
     assert 0 < types <= 144
     assert info["lib_types"] == types and info["failed"] == 0
+
+
+@pytest.mark.timeout(900)
+def test_group_type_library_bands(lib):
+    """A mix with more group types than one library holds gets several libraries (compiled in parallel on the
+    host): the 16 most swept types in each and a band of 16 more, up to 144 distinct types."""
+    progs = []
+    for s in range(6):
+        n = 18 + s % 3
+        prog, _, _ = q.compile_circuit(gen.random_layer_ccx(n, 12, 90 + s), n, 12)
+        progs += [(seg, n) for kind, seg in prog if kind == "segment"]
+    old = engine.set_jit("library")
+    try:
+        types = engine.jit_prepare_library(progs)
+        info = engine.jit_info()
+    finally:
+        engine.set_jit(old)
+    assert 32 < types <= 144, types
+    assert info["lib_types"] == types and info["failed"] == 0
