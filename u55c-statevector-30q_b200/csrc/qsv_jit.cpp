@@ -178,7 +178,7 @@ struct Jit {
     bool stopping = false;      // set at process exit: workers take no new work
     int mode = 2;
     long long jit_launches = 0, interp_launches = 0, coarse_launches = 0, compiled = 0, failed = 0;
-    // group-type library: amplitudes swept per group type, the library in use and the one being built
+    // group-type libraries: amplitudes swept per group type, the set in use and the one being built
     std::unordered_map<std::string, double> gweight;
     std::shared_ptr<LibSet> lib, lib_next;
     double lib_uncovered = 0.0;
@@ -308,10 +308,11 @@ std::string gen_source_stream(const QsvSweep &sw, int rb, int wb) {
 // ---------------------------------------------------------------- group-type library
 // Sweeps whose exact and coarse structures never repeat (random gate choices, random Toffoli positions)
 // still repeat at the level of one group of the streaming form: the op sequence of a group (per op: slot
-// among the item bits, variant, kind, matrix classes, r00) recurs across sweeps and circuits. The library
-// is ONE kernel for 13-qubit windows with straight-line code for each of up to kLibMaxTypes group types and
-// a run-time-dispatch path for the others; it is rebuilt, in the background, from the types that have
-// swept the most amplitudes. Item bits, control masks and matrices are read at run time.
+// among the item bits, variant, kind, matrix classes, r00) recurs across sweeps and circuits. A library
+// is ONE kernel for 13-qubit windows with straight-line code for each of its group types and a
+// run-time-dispatch path for the others, selected per group; a set of libraries is rebuilt, in the
+// background, from the types that have swept the most amplitudes. Item bits, control masks and matrices
+// are read at run time.
 // A library holds kLibCommon + kLibBand cases: front-end compile time grows faster than linearly with the
 // cases (10 / 20 / 40 / 86 cases: 4 / 7 / 17 / ~80 s), so wider coverage comes from several libraries
 // compiled in parallel. The 16 / 64 most swept group types cover 87 / 94 % of the groups of a mixed batch.
@@ -763,7 +764,8 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
     std::unique_lock<std::mutex> lk(j.mu);
     std::vector<std::shared_ptr<Entry>> mine;
     if (j.mode == 4 && !stream_form()) {
-        // group-type library: one build (blocking) that covers every group type of the 13-qubit sweeps
+        // group-type libraries: one build (blocking) from the group types of the 13-qubit sweeps (the most
+        // swept 144 of them, these first)
         int rb = 0, wb = 0;
         layout_for_kw(13, &rb, &wb);
         std::vector<QsvSweep> s13;
@@ -820,8 +822,8 @@ int jit_prepare(const std::vector<QsvSweep> &sweeps) {
 }
 
 // Build (blocking) a group-type library from the 13-qubit sweeps of many programs: their group types'
-// swept amplitudes are recorded and the library takes the kLibMaxTypes most swept of every type seen so far.
-// Returns the number of types in the library in use, or -1 if the build failed.
+// swept amplitudes are recorded and the libraries take the most swept of every type seen so far (lib_build).
+// Returns the number of distinct types in the libraries in use, or -1 if a library failed to compile.
 int jit_prepare_library(const std::vector<QsvSweep> &sweeps) {
     Jit &j = J();
     std::unique_lock<std::mutex> lk(j.mu);
