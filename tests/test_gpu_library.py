@@ -1,9 +1,10 @@
 """The group-type library kernel gives the C oracle's values exactly.
 
 The library (qsv_set_jit mode 4, "library") is a set of kernels for 13-qubit windows (up to 8, each with the
-16 most swept group types and a band of 16 more), each with straight-line code for its group types of the streaming form (per op: slot among the group's item bits, variant, kind, matrix
-classes) and a run-time-dispatch path for groups of other types; item bits, control masks and matrices are
-read at run time. Its cases and its fallback run the interpreter's per-variant arithmetic, so every value
+16 most swept group types and a band of 16 more), each with straight-line code for its group types of the
+streaming form (per op: slot among the group's item bits, variant, kind, matrix classes) and a
+run-time-dispatch path for groups of other types; item bits, control masks and matrices are read at run
+time. Its cases and its fallback run the interpreter's per-variant arithmetic, so every value
 equals the oracle's (np.array_equal: signs of zeros aside). Cases: random layers with Toffolis (controls on
 item and base bits), random circuits, VQE (CX chains), the zoo (every gate family), QFT (diagonal runs),
 Grover (wide multi-controlled gates); a library built from one circuit serving another (groups in cases and
